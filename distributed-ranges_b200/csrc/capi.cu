@@ -1,0 +1,580 @@
+// capi.cu -- the extern "C" entry points declared in include/drb.h.
+//
+// The handle (drb_csr_t) plays the role of the reference's
+// distributed_sparse_matrix + csr_row_distribution / csr_eq_distribution:
+// it owns device copies of the CSR arrays (csr_row_distribution.hpp:205-318
+// copies each rank's slice into MPI-window memory; here all slices are one
+// device allocation), the row-block plan, and the segment table that
+// segments() reports.  No exception crosses the ABI.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+#include "drb_internal.cuh"
+
+namespace drb {
+
+int plan_group(int vbytes, int cbytes);
+
+std::atomic<uint64_t> g_launch_count{0};
+
+namespace {
+thread_local std::string t_error;
+
+struct DeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) {
+      switched = cudaSetDevice(dev) == cudaSuccess;
+    }
+  }
+  ~DeviceGuard() {
+    if (switched)
+      cudaSetDevice(prev);
+  }
+};
+
+drb_status invalid(const char *msg) {
+  set_error("invalid argument: %s", msg);
+  return DRB_ERR_INVALID_ARG;
+}
+
+drb_status check_device(int *dev) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    set_error("no CUDA device available (%s)",
+              e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+    return DRB_ERR_NO_DEVICE;
+  }
+  DRB_CUDA_TRY(cudaGetDevice(dev));
+  cudaDeviceProp prop;
+  DRB_CUDA_TRY(cudaGetDeviceProperties(&prop, *dev));
+  if (prop.major != 10 || prop.minor != 0) {
+    set_error("device %d is sm_%d%d; this library is built for sm_100a (B200)",
+              *dev, prop.major, prop.minor);
+    return DRB_ERR_NO_DEVICE;
+  }
+  return DRB_OK;
+}
+
+template <class I>
+drb_status validate_rowptr(const I *rp, int64_t m, int64_t nnz) {
+  if ((int64_t)rp[0] != 0) {
+    set_error("bad CSR: rowptr[0] = %lld, expected 0", (long long)rp[0]);
+    return DRB_ERR_BAD_CSR;
+  }
+  for (int64_t i = 0; i < m; i++) {
+    if (rp[i + 1] < rp[i]) {
+      set_error("bad CSR: rowptr decreases at row %lld", (long long)i);
+      return DRB_ERR_BAD_CSR;
+    }
+  }
+  if ((int64_t)rp[m] != nnz) {
+    set_error("bad CSR: rowptr[m] = %lld but nnz = %lld", (long long)rp[m],
+              (long long)nnz);
+    return DRB_ERR_BAD_CSR;
+  }
+  return DRB_OK;
+}
+
+template <class I>
+drb_status validate_cols(const I *ci, int64_t nnz, int64_t n) {
+  const int64_t nth =
+      nnz > (1 << 22) ? std::min<int64_t>(16, std::max(1u, std::thread::hardware_concurrency())) : 1;
+  std::vector<int64_t> bad(nth, -1);
+  auto work = [&](int64_t t) {
+    const int64_t lo = nnz * t / nth, hi = nnz * (t + 1) / nth;
+    for (int64_t p = lo; p < hi; p++) {
+      const int64_t c = (int64_t)ci[p];
+      if (c < 0 || c >= n) {
+        bad[t] = p;
+        return;
+      }
+    }
+  };
+  if (nth == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int64_t t = 0; t < nth; t++)
+      th.emplace_back(work, t);
+    for (auto &t : th)
+      t.join();
+  }
+  for (int64_t t = 0; t < nth; t++)
+    if (bad[t] >= 0) {
+      set_error("bad CSR: column index %lld at nnz %lld is outside [0, %lld)",
+                (long long)ci[bad[t]], (long long)bad[t], (long long)n);
+      return DRB_ERR_BAD_CSR;
+    }
+  return DRB_OK;
+}
+
+int64_t rp_at(const void *rp, int ib, int64_t i) {
+  return ib == 8 ? ((const int64_t *)rp)[i] : (int64_t)((const int32_t *)rp)[i];
+}
+
+// Upload `count` elements of width in_b to dst (width out_b), narrowing or
+// widening on the device through a temporary when the widths differ.
+drb_status upload(void *dst, int out_b, const void *src, int in_b,
+                  int64_t count, bool src_on_device, bool to_bf16,
+                  cudaStream_t s) {
+  if (count == 0)
+    return DRB_OK;
+  const cudaMemcpyKind kind =
+      src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (in_b == out_b && !to_bf16) {
+    DRB_CUDA_TRY(cudaMemcpyAsync(dst, src, (size_t)in_b * count, kind, s));
+    return DRB_OK;
+  }
+  const void *dsrc = src;
+  DevBuf tmp;
+  if (!src_on_device) {
+    DRB_TRY(tmp.alloc((size_t)in_b * count));
+    DRB_CUDA_TRY(cudaMemcpyAsync(tmp.p, src, (size_t)in_b * count, kind, s));
+    dsrc = tmp.p;
+  }
+  DRB_TRY(convert_launch(dsrc, in_b, dst, out_b, count, to_bf16, s));
+  DRB_CUDA_TRY(cudaStreamSynchronize(s)); // tmp is freed on return
+  return DRB_OK;
+}
+
+void compute_segments(Csr &A, const void *rp, int ib) {
+  const int64_t P = A.nseg, m = A.m, nnz = A.nnz;
+  A.seg_row0.assign(P, 0);
+  A.seg_row1.assign(P, 0);
+  A.seg_nz0.assign(P, 0);
+  A.seg_nz1.assign(P, 0);
+  if (A.part == DRB_PART_ROW) {
+    // distributed_vector<I>(m) segment size ceil(m/P)
+    // (distributed_vector.hpp:310); nnz ranges per
+    // csr_row_distribution.hpp:234-252.
+    const int64_t seg = (m + P - 1) / P;
+    for (int64_t r = 0; r < P; r++) {
+      const int64_t r0 = std::min(m, r * seg), r1 = std::min(m, (r + 1) * seg);
+      A.seg_row0[r] = r0;
+      A.seg_row1[r] = r1;
+      A.seg_nz0[r] = rp_at(rp, ib, r0);
+      A.seg_nz1[r] = rp_at(rp, ib, r1);
+    }
+  } else {
+    // distributed_vector<T>(nnz) segment size ceil(nnz/P); the rows a
+    // segment touches come from upper_bound over rowptr[0..m)
+    // (csr_eq_distribution.hpp:253-272).
+    const int64_t seg = (nnz + P - 1) / P;
+    auto ub = [&](int64_t v) {
+      int64_t lo = 0, hi = m;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (rp_at(rp, ib, mid) <= v)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      return lo;
+    };
+    for (int64_t r = 0; r < P; r++) {
+      const int64_t z0 = std::min(nnz, r * seg), z1 = std::min(nnz, (r + 1) * seg);
+      A.seg_nz0[r] = z0;
+      A.seg_nz1[r] = z1;
+      if (z0 >= z1) {
+        A.seg_row0[r] = A.seg_row1[r] = m;
+        continue;
+      }
+      A.seg_row0[r] = std::max<int64_t>(0, ub(z0) - 1);
+      A.seg_row1[r] = ub(z1 - 1);
+    }
+  }
+}
+
+} // namespace
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  t_error = buf;
+}
+void clear_error() { t_error.clear(); }
+
+drb_status DevBuf::alloc(size_t nbytes) {
+  release();
+  if (nbytes == 0)
+    nbytes = 16;
+  cudaError_t e = cudaMalloc(&p, nbytes);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    set_error("cudaMalloc(%zu) failed: %s", nbytes, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? DRB_ERR_OOM : DRB_ERR_CUDA;
+  }
+  bytes = nbytes;
+  return DRB_OK;
+}
+
+drb_status DevBuf::ensure(size_t nbytes) {
+  if (p && bytes >= nbytes)
+    return DRB_OK;
+  return alloc(nbytes);
+}
+
+void DevBuf::release() {
+  if (p)
+    cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+Csr::~Csr() = default;
+
+} // namespace drb
+
+using namespace drb;
+
+struct drb_csr_matrix : public Csr {};
+
+extern "C" {
+
+const char *drb_last_error(void) { return t_error.c_str(); }
+
+const char *drb_version(void) { return "drb 0.1 (sm_100a)"; }
+
+uint64_t drb_launch_count(void) { return g_launch_count.load(); }
+
+drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
+                          const void *rowptr, const void *colind,
+                          const void *values, drb_itype index_type,
+                          drb_dtype value_type, drb_dtype storage,
+                          int nsegments, drb_partition partition,
+                          uint32_t flags, void *stream) {
+  clear_error();
+  if (!out)
+    return invalid("out is NULL");
+  *out = nullptr;
+  if (m < 0 || n < 0 || nnz < 0)
+    return invalid("negative m, n or nnz");
+  if (m >= 0x7fffffff) {
+    set_error("m = %lld rows: at most 2^31-2 rows per handle", (long long)m);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  if (!rowptr)
+    return invalid("rowptr is NULL");
+  if (nnz > 0 && (!colind || !values))
+    return invalid("colind or values is NULL");
+  if (index_type != DRB_I32 && index_type != DRB_I64)
+    return invalid("index_type");
+  if (value_type != DRB_F32 && value_type != DRB_F64)
+    return invalid("value_type must be DRB_F32 or DRB_F64");
+  if (!(storage == value_type || (storage == DRB_BF16 && value_type == DRB_F32)))
+    return invalid("storage must equal value_type, or be DRB_BF16 for F32");
+  if (nsegments < 1)
+    return invalid("nsegments < 1");
+  if (partition != DRB_PART_ROW && partition != DRB_PART_EQ)
+    return invalid("partition");
+  if (index_type == DRB_I32 && (nnz > 0x7fffffff || n > 0x7fffffff))
+    return invalid("int32 indices cannot address nnz or n >= 2^31");
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool on_dev = flags & DRB_FLAG_DEVICE_INPUT;
+  const int ib = index_type == DRB_I64 ? 8 : 4;
+
+  std::vector<char> rp_copy;
+  const void *rp_h = rowptr;
+  if (on_dev) {
+    rp_copy.resize((size_t)ib * (m + 1));
+    DRB_CUDA_TRY(cudaMemcpy(rp_copy.data(), rowptr, rp_copy.size(),
+                            cudaMemcpyDeviceToHost));
+    rp_h = rp_copy.data();
+  }
+  if (!(flags & DRB_FLAG_SKIP_VALIDATE)) {
+    if (ib == 8)
+      DRB_TRY(validate_rowptr((const int64_t *)rp_h, m, nnz));
+    else
+      DRB_TRY(validate_rowptr((const int32_t *)rp_h, m, nnz));
+    if (!on_dev) {
+      if (ib == 8)
+        DRB_TRY(validate_cols((const int64_t *)colind, nnz, n));
+      else
+        DRB_TRY(validate_cols((const int32_t *)colind, nnz, n));
+    }
+  } else if (rp_at(rp_h, ib, m) != nnz) {
+    set_error("bad CSR: rowptr[m] != nnz");
+    return DRB_ERR_BAD_CSR;
+  }
+
+  auto A = std::make_unique<drb_csr_matrix>();
+  A->device = dev;
+  A->m = m;
+  A->n = n;
+  A->nnz = nnz;
+  A->value_type = value_type;
+  A->storage = storage;
+  A->nseg = nsegments;
+  A->part = partition;
+  A->flags = flags;
+  A->cbytes = (ib == 8 && ((flags & DRB_FLAG_KEEP_INDEX64) || n > 0x7fffffff)) ? 8 : 4;
+  A->rbytes = (ib == 8 && ((flags & DRB_FLAG_KEEP_INDEX64) || nnz > 0x7fffffff)) ? 8 : 4;
+  const int vb_in = dtype_bytes(value_type), vb = dtype_bytes(storage);
+  const int64_t pad = ((nnz + kPadElems - 1) / kPadElems + 1) * kPadElems;
+  DRB_TRY(A->rowptr.alloc((size_t)A->rbytes * (m + 1)));
+  DRB_TRY(A->colind.alloc((size_t)A->cbytes * pad));
+  DRB_TRY(A->vals.alloc((size_t)vb * pad));
+  DRB_CUDA_TRY(cudaMemsetAsync(A->colind.p, 0, A->colind.bytes, s));
+  DRB_CUDA_TRY(cudaMemsetAsync(A->vals.p, 0, A->vals.bytes, s));
+  DRB_TRY(upload(A->rowptr.p, A->rbytes, rowptr, ib, m + 1, on_dev, false, s));
+  DRB_TRY(upload(A->colind.p, A->cbytes, colind, ib, nnz, on_dev, false, s));
+  DRB_TRY(upload(A->vals.p, vb, values, vb_in, nnz, on_dev,
+                 storage == DRB_BF16, s));
+  DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  DRB_TRY(build_plan(A->plan, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0, 0));
+  compute_segments(*A, rp_h, ib);
+  if (flags & DRB_FLAG_ADJOINT) {
+    DRB_TRY(adjoint_build(*A, s));
+    DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  *out = A.release();
+  return DRB_OK;
+}
+
+drb_status drb_csr_destroy(drb_csr_t A) {
+  clear_error();
+  if (!A)
+    return DRB_OK;
+  DeviceGuard g(A->device);
+  cudaDeviceSynchronize();
+  delete A;
+  return DRB_OK;
+}
+
+drb_status drb_csr_shape(drb_csr_t A, int64_t *m, int64_t *n, int64_t *nnz) {
+  if (!A)
+    return invalid("A is NULL");
+  if (m)
+    *m = A->m;
+  if (n)
+    *n = A->n;
+  if (nnz)
+    *nnz = A->nnz;
+  return DRB_OK;
+}
+
+drb_status drb_csr_storage(drb_csr_t A, int *value_bytes, int *col_bytes,
+                           int *rowptr_bytes) {
+  if (!A)
+    return invalid("A is NULL");
+  if (value_bytes)
+    *value_bytes = dtype_bytes(A->storage);
+  if (col_bytes)
+    *col_bytes = A->cbytes;
+  if (rowptr_bytes)
+    *rowptr_bytes = A->rbytes;
+  return DRB_OK;
+}
+
+drb_status drb_csr_num_segments(drb_csr_t A, int *nsegments) {
+  if (!A || !nsegments)
+    return invalid("NULL argument");
+  *nsegments = A->nseg;
+  return DRB_OK;
+}
+
+drb_status drb_csr_segment(drb_csr_t A, int seg, int64_t *row_begin,
+                           int64_t *row_end, int64_t *nnz_begin,
+                           int64_t *nnz_end) {
+  if (!A)
+    return invalid("A is NULL");
+  if (seg < 0 || seg >= A->nseg)
+    return invalid("segment index out of range");
+  if (row_begin)
+    *row_begin = A->seg_row0[seg];
+  if (row_end)
+    *row_end = A->seg_row1[seg];
+  if (nnz_begin)
+    *nnz_begin = A->seg_nz0[seg];
+  if (nnz_end)
+    *nnz_end = A->seg_nz1[seg];
+  return DRB_OK;
+}
+
+drb_status drb_csr_get_entries(drb_csr_t A, int64_t offset, int64_t count,
+                               int64_t *rows, int64_t *cols, double *values) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  if (offset < 0 || count < 0 || offset + count > A->nnz)
+    return invalid("entry range outside [0, nnz)");
+  if (count == 0)
+    return DRB_OK;
+  DeviceGuard g(A->device);
+  if (rows) {
+    if (A->rowptr_h.empty()) {
+      std::vector<char> raw((size_t)A->rbytes * (A->m + 1));
+      DRB_CUDA_TRY(cudaMemcpy(raw.data(), A->rowptr.p, raw.size(),
+                              cudaMemcpyDeviceToHost));
+      A->rowptr_h.resize(A->m + 1);
+      for (int64_t i = 0; i <= A->m; i++)
+        A->rowptr_h[i] = rp_at(raw.data(), A->rbytes, i);
+    }
+    const auto &rp = A->rowptr_h;
+    int64_t r = std::upper_bound(rp.begin(), rp.end(), offset) - rp.begin() - 1;
+    for (int64_t i = 0; i < count; i++) {
+      while (rp[r + 1] <= offset + i)
+        r++;
+      rows[i] = r;
+    }
+  }
+  if (cols) {
+    std::vector<char> raw((size_t)A->cbytes * count);
+    DRB_CUDA_TRY(cudaMemcpy(raw.data(),
+                            (const char *)A->colind.p + (size_t)A->cbytes * offset,
+                            raw.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < count; i++)
+      cols[i] = rp_at(raw.data(), A->cbytes, i);
+  }
+  if (values) {
+    const int vb = dtype_bytes(A->storage);
+    std::vector<char> raw((size_t)vb * count);
+    DRB_CUDA_TRY(cudaMemcpy(raw.data(),
+                            (const char *)A->vals.p + (size_t)vb * offset,
+                            raw.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < count; i++) {
+      if (A->storage == DRB_F64) {
+        values[i] = ((const double *)raw.data())[i];
+      } else if (A->storage == DRB_F32) {
+        values[i] = ((const float *)raw.data())[i];
+      } else {
+        uint32_t u = (uint32_t)((const uint16_t *)raw.data())[i] << 16;
+        float f;
+        std::memcpy(&f, &u, 4);
+        values[i] = f;
+      }
+    }
+  }
+  return DRB_OK;
+}
+
+drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
+                        drb_layout layout, void *stream) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  if (k < 1)
+    return invalid("k < 1");
+  if (layout != DRB_COL_MAJOR && layout != DRB_ROW_MAJOR)
+    return invalid("layout");
+  if ((A->m > 0 && !y) || (A->n > 0 && A->nnz > 0 && !x))
+    return invalid("x or y is NULL");
+  if (A->m == 0)
+    return DRB_OK;
+  DeviceGuard g(A->device);
+  return spmv_launch(*A, x, y, k, layout, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
+                             int64_t k, drb_layout layout, void *stream) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  if (k < 1)
+    return invalid("k < 1");
+  if ((A->m > 0 && !y_host) || (A->n > 0 && !x_host))
+    return invalid("x or y is NULL");
+  if (A->m == 0)
+    return DRB_OK;
+  DeviceGuard g(A->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t xb = (size_t)(A->storage == DRB_BF16 ? 2 : dtype_bytes(A->storage));
+  const size_t yb = (size_t)(A->storage == DRB_BF16 ? 4 : dtype_bytes(A->storage));
+  DRB_TRY(A->xh_dev.ensure(xb * A->n * k));
+  DRB_TRY(A->yh_dev.ensure(yb * A->m * k));
+  if (A->n > 0)
+    DRB_CUDA_TRY(cudaMemcpyAsync(A->xh_dev.p, x_host, xb * A->n * k,
+                                 cudaMemcpyHostToDevice, s));
+  DRB_TRY(spmv_launch(*A, A->xh_dev.p, A->yh_dev.p, k, layout, s));
+  DRB_CUDA_TRY(cudaMemcpyAsync(y_host, A->yh_dev.p, yb * A->m * k,
+                               cudaMemcpyDeviceToHost, s));
+  DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  return DRB_OK;
+}
+
+drb_status drb_csr_residual_norm2(drb_csr_t A, const void *x, const void *b,
+                                  void *y, double *out, void *stream) {
+  clear_error();
+  if (!A || !out || (A->m > 0 && !b) || (A->nnz > 0 && !x))
+    return invalid("NULL argument");
+  if (A->storage == DRB_BF16)
+    return invalid("residual_norm2 takes F32 or F64 storage");
+  DeviceGuard g(A->device);
+  return residual_launch(*A, x, b, y, out, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
+                                 void *xbar, void *abar, void *stream) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  if (!A->has_adjoint) {
+    set_error("gemv_backward needs a handle created with DRB_FLAG_ADJOINT");
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (!ybar && (xbar || abar))
+    return invalid("ybar is NULL");
+  if (abar && !x)
+    return invalid("x is NULL but abar requested");
+  DeviceGuard g(A->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (xbar && A->n > 0)
+    DRB_TRY(spmv_t_launch(*A, ybar, xbar, s));
+  if (abar && A->nnz > 0)
+    DRB_TRY(abar_launch(*A, ybar, x, abar, s));
+  return DRB_OK;
+}
+
+drb_status drb_csr_update_values(drb_csr_t A, const void *values,
+                                 void *stream) {
+  clear_error();
+  if (!A || (A->nnz > 0 && !values))
+    return invalid("NULL argument");
+  DeviceGuard g(A->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (A->nnz == 0)
+    return DRB_OK;
+  DRB_CUDA_TRY(cudaMemcpyAsync(A->vals.p, values,
+                               (size_t)dtype_bytes(A->storage) * A->nnz,
+                               cudaMemcpyDeviceToDevice, s));
+  return adjoint_refresh_values(*A, s);
+}
+
+drb_status drb_dense_gemv(int64_t m, int64_t n, const void *Am, int64_t lda,
+                          const void *x, void *y, int64_t k, drb_layout layout,
+                          drb_dtype dtype, void *stream) {
+  clear_error();
+  if (m < 0 || n < 0 || k < 1 || lda < n)
+    return invalid("sizes (need m, n >= 0, k >= 1, lda >= n)");
+  if ((m > 0 && n > 0 && (!Am || !x)) || (m > 0 && !y))
+    return invalid("NULL pointer");
+  if (layout != DRB_COL_MAJOR && layout != DRB_ROW_MAJOR)
+    return invalid("layout");
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  return dense_launch(m, n, Am, lda, x, y, k, layout, dtype,
+                      static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
+                   double *out, void *stream) {
+  clear_error();
+  if (n < 0 || !out || (n > 0 && (!a || !b)))
+    return invalid("NULL pointer or negative n");
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  return dot_launch(n, a, b, dtype, out, static_cast<cudaStream_t>(stream));
+}
+
+} // extern "C"

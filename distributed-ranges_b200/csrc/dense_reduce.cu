@@ -1,0 +1,277 @@
+// dense_reduce.cu -- dense row-major gemv and the deterministic dot/norm
+// reduction.
+//
+// Dense gemv has no dr::mp counterpart (dr::mp::gemv only takes
+// distributed_sparse_matrix, include/dr/mp/algorithms/matrix/gemv.hpp:16-71);
+// it is shaped after the sparse call over a row-major matrix, the layout of
+// dr::sp::distributed_dense_matrix tiles
+// (include/dr/sp/containers/distributed_dense_matrix.hpp:205-219).
+// The dot product replaces mp::reduce over zip(a, b) | transform(mul)
+// (include/dr/mp/algorithms/reduce.hpp:58-107,
+// benchmarks/gbench/common/dot_product.cpp:33-52) with one launch and a
+// fixed summation order.
+#include "drb_internal.cuh"
+
+namespace drb {
+namespace {
+
+constexpr int kDenseNT = 256;
+
+template <class V> __device__ __forceinline__ V warp_sum_d(V v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// One warp owns RPW consecutive rows at a time and streams them with 16-byte
+// loads (evict-first); x is read through L1 once per column step and reused
+// for the RPW rows and KB right-hand sides.  x is column-major (x[c + j*n]).
+template <class V, int KB, int RPW, bool VEC>
+__global__ void __launch_bounds__(kDenseNT)
+    dense_gemv_kernel(int64_t m, int64_t n, const V *__restrict__ A,
+                      int64_t lda, const V *__restrict__ x,
+                      V *__restrict__ y, int64_t kb_count, int64_t y_ld,
+                      int64_t y_js) {
+  constexpr int PER = 16 / sizeof(V);
+  const uint64_t pol_s = ptx::policy_evict_first();
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * kDenseNT + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * kDenseNT) >> 5;
+  const int64_t nvec = VEC ? (n / PER) * PER : 0;
+  for (int64_t row0 = warp * RPW; row0 < m; row0 += nwarps * RPW) {
+    V acc[RPW][KB];
+#pragma unroll
+    for (int r = 0; r < RPW; r++)
+#pragma unroll
+      for (int j = 0; j < KB; j++)
+        acc[r][j] = 0;
+    if (VEC) {
+      for (int64_t c = (int64_t)lane * PER; c < nvec; c += 32 * PER) {
+        V a[RPW][PER];
+#pragma unroll
+        for (int r = 0; r < RPW; r++) {
+          union {
+            uint4 u;
+            V t[PER];
+          } w;
+          w.u = make_uint4(0, 0, 0, 0);
+          if (row0 + r < m)
+            w.u = ptx::ld_stream16(A + (row0 + r) * lda + c, pol_s);
+#pragma unroll
+          for (int i = 0; i < PER; i++)
+            a[r][i] = w.t[i];
+        }
+#pragma unroll
+        for (int j = 0; j < KB; j++) {
+          union {
+            uint4 u;
+            V t[PER];
+          } xv;
+          xv.u = __ldg(reinterpret_cast<const uint4 *>(x + j * n + c));
+#pragma unroll
+          for (int r = 0; r < RPW; r++)
+#pragma unroll
+            for (int i = 0; i < PER; i++)
+              acc[r][j] += a[r][i] * xv.t[i];
+        }
+      }
+    }
+    for (int64_t c = nvec + lane; c < n; c += 32) {
+#pragma unroll
+      for (int j = 0; j < KB; j++) {
+        const V xv = __ldg(x + j * n + c);
+#pragma unroll
+        for (int r = 0; r < RPW; r++)
+          if (row0 + r < m)
+            acc[r][j] += A[(row0 + r) * lda + c] * xv;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < RPW; r++)
+#pragma unroll
+      for (int j = 0; j < KB; j++) {
+        const V s = warp_sum_d(acc[r][j]);
+        if (lane == 0 && row0 + r < m && j < kb_count)
+          y[(row0 + r) * y_ld + j * y_js] = s;
+      }
+  }
+}
+
+template <class V, int KB, int RPW>
+void dense_call(bool vec, unsigned grid, cudaStream_t s, int64_t m, int64_t n,
+                const V *A, int64_t lda, const V *x, V *y, int64_t kbc,
+                int64_t y_ld, int64_t y_js) {
+  if (vec)
+    dense_gemv_kernel<V, KB, RPW, true><<<grid, kDenseNT, 0, s>>>(
+        m, n, A, lda, x, y, kbc, y_ld, y_js);
+  else
+    dense_gemv_kernel<V, KB, RPW, false><<<grid, kDenseNT, 0, s>>>(
+        m, n, A, lda, x, y, kbc, y_ld, y_js);
+  note_launch();
+}
+
+template <class V>
+drb_status dense_typed(int64_t m, int64_t n, const V *A, int64_t lda,
+                       const V *x, V *y, int64_t k, drb_layout layout,
+                       cudaStream_t s) {
+  constexpr int PER = 16 / sizeof(V);
+  // x as column-major: a row-major k > 1 block is transposed first.
+  const V *xc = x;
+  void *tmp = nullptr;
+  if (layout == DRB_ROW_MAJOR && k > 1) {
+    DRB_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(V) * n * k, s));
+    drb_status st = transpose_launch(x, tmp, n, k, sizeof(V), s);
+    if (st != DRB_OK) {
+      cudaFreeAsync(tmp, s);
+      return st;
+    }
+    xc = static_cast<const V *>(tmp);
+  }
+  const bool vec = (reinterpret_cast<uintptr_t>(A) % 16 == 0) &&
+                   (reinterpret_cast<uintptr_t>(xc) % 16 == 0) &&
+                   (lda % PER == 0) && (n % PER == 0);
+  const unsigned grid = 148 * 8;
+  // y address of (row r, rhs j): r*y_ld + j*y_js
+  const int64_t y_ld = layout == DRB_ROW_MAJOR ? k : 1;
+  const int64_t y_js = layout == DRB_ROW_MAJOR ? 1 : m;
+  for (int64_t jb = 0; jb < k;) {
+    const int64_t left = k - jb;
+    const V *xj = xc + jb * n;
+    V *yj = y + jb * y_js;
+    if (left >= 8) {
+      dense_call<V, 8, 1>(vec, grid, s, m, n, A, lda, xj, yj, 8, y_ld, y_js);
+      jb += 8;
+    } else if (left >= 4) {
+      dense_call<V, 4, 2>(vec, grid, s, m, n, A, lda, xj, yj, 4, y_ld, y_js);
+      jb += 4;
+    } else if (left >= 2) {
+      dense_call<V, 2, 2>(vec, grid, s, m, n, A, lda, xj, yj, 2, y_ld, y_js);
+      jb += 2;
+    } else {
+      dense_call<V, 1, 4>(vec, grid, s, m, n, A, lda, xj, yj, 1, y_ld, y_js);
+      jb += 1;
+    }
+  }
+  cudaError_t e = cudaGetLastError();
+  if (tmp)
+    cudaFreeAsync(tmp, s);
+  if (e != cudaSuccess) {
+    set_error("dense gemv launch: %s", cudaGetErrorString(e));
+    return DRB_ERR_CUDA;
+  }
+  return DRB_OK;
+}
+
+// ---- dot -------------------------------------------------------------------------
+constexpr int kDotNT = 256;
+constexpr int kDotGrid = 296; // fixed: the summation order must not vary
+
+template <class V>
+__global__ void __launch_bounds__(kDotNT)
+    dot_kernel(int64_t n, const V *__restrict__ a, const V *__restrict__ b,
+               double *partials, int *ticket, double *out) {
+  __shared__ double s_red[kDotNT / 32];
+  __shared__ int s_last;
+  constexpr int PER = 16 / sizeof(V);
+  const uint64_t pol_s = ptx::policy_evict_first();
+  double acc = 0.0;
+  const int64_t tid = (int64_t)blockIdx.x * kDotNT + threadIdx.x;
+  const int64_t nth = (int64_t)gridDim.x * kDotNT;
+  const bool vec = (reinterpret_cast<uintptr_t>(a) % 16 == 0) &&
+                   (reinterpret_cast<uintptr_t>(b) % 16 == 0);
+  int64_t done = 0;
+  if (vec) {
+    const int64_t nv = n / PER;
+    for (int64_t i = tid; i < nv; i += nth) {
+      union {
+        uint4 u;
+        V t[PER];
+      } wa, wb;
+      wa.u = ptx::ld_stream16(a + i * PER, pol_s);
+      wb.u = (a == b) ? wa.u : ptx::ld_stream16(b + i * PER, pol_s);
+#pragma unroll
+      for (int q = 0; q < PER; q++)
+        acc += (double)wa.t[q] * (double)wb.t[q];
+    }
+    done = nv * PER;
+  }
+  for (int64_t i = done + tid; i < n; i += nth)
+    acc += (double)a[i] * (double)b[i];
+  // block reduction
+  acc = warp_sum_d(acc);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+    s_red[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kDotNT / 32; w++)
+      s += s_red[w];
+    partials[blockIdx.x] = s;
+    __threadfence();
+    s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    double s = 0.0;
+    for (int i = 0; i < (int)gridDim.x; i++)
+      s += *(volatile double *)&partials[i];
+    *out = s;
+    *ticket = 0;
+  }
+}
+
+} // namespace
+
+drb_status dense_launch(int64_t m, int64_t n, const void *A, int64_t lda,
+                        const void *x, void *y, int64_t k, drb_layout layout,
+                        drb_dtype dt, cudaStream_t s) {
+  if (m == 0 || k == 0)
+    return DRB_OK;
+  if (n == 0) {
+    DRB_CUDA_TRY(cudaMemsetAsync(y, 0, (size_t)dtype_bytes(dt) * m * k, s));
+    return DRB_OK;
+  }
+  if (dt == DRB_F32)
+    return dense_typed<float>(m, n, (const float *)A, lda, (const float *)x,
+                              (float *)y, k, layout, s);
+  if (dt == DRB_F64)
+    return dense_typed<double>(m, n, (const double *)A, lda, (const double *)x,
+                               (double *)y, k, layout, s);
+  set_error("dense gemv: dtype %d not supported", (int)dt);
+  return DRB_ERR_UNSUPPORTED;
+}
+
+drb_status dot_launch(int64_t n, const void *a, const void *b, drb_dtype dt,
+                      double *out, cudaStream_t s) {
+  if (dt != DRB_F32 && dt != DRB_F64) {
+    set_error("dot: dtype %d not supported", (int)dt);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  void *scratch = nullptr;
+  const size_t bytes = sizeof(double) * kDotGrid + 16;
+  DRB_CUDA_TRY(cudaMallocAsync(&scratch, bytes, s));
+  double *partials = static_cast<double *>(scratch);
+  int *ticket = reinterpret_cast<int *>(partials + kDotGrid);
+  cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(int), s);
+  if (e == cudaSuccess) {
+    if (dt == DRB_F32)
+      dot_kernel<float><<<kDotGrid, kDotNT, 0, s>>>(
+          n, (const float *)a, (const float *)b, partials, ticket, out);
+    else
+      dot_kernel<double><<<kDotGrid, kDotNT, 0, s>>>(
+          n, (const double *)a, (const double *)b, partials, ticket, out);
+    note_launch();
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(scratch, s);
+  if (e != cudaSuccess) {
+    set_error("dot launch: %s", cudaGetErrorString(e));
+    return DRB_ERR_CUDA;
+  }
+  return DRB_OK;
+}
+
+} // namespace drb

@@ -1,0 +1,201 @@
+// drb_internal.cuh -- shared declarations of the drb CUDA library.
+//
+// Data layout in HBM (one handle = one CSR matrix, all segments on one GPU):
+//   rowptr  [m+1]   int32 when nnz < 2^31, else int64
+//   colind  [nnz]   int32 when n < 2^31 (unless DRB_FLAG_KEEP_INDEX64)
+//   values  [nnz]   f32 | f64 | bf16
+// colind/values are padded to a multiple of kPadElems with zeros so that the
+// 16-byte vector loads of a row-block tile may read past the last nonzero.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "drb.h"
+
+namespace drb {
+
+// ---- errors ----------------------------------------------------------------
+void set_error(const char *fmt, ...);
+void clear_error();
+
+#define DRB_CUDA_TRY(...)                                                     \
+  do {                                                                         \
+    cudaError_t e_ = (__VA_ARGS__);                                                 \
+    if (e_ != cudaSuccess) {                                                   \
+      ::drb::set_error("%s failed: %s (%s:%d)", #__VA_ARGS__, cudaGetErrorString(e_), \
+                       __FILE__, __LINE__);                                    \
+      return e_ == cudaErrorMemoryAllocation ? DRB_ERR_OOM : DRB_ERR_CUDA;     \
+    }                                                                          \
+  } while (0)
+
+#define DRB_TRY(...)                                                          \
+  do {                                                                         \
+    drb_status s_ = (__VA_ARGS__);                                                  \
+    if (s_ != DRB_OK)                                                          \
+      return s_;                                                               \
+  } while (0)
+
+// Every kernel launch goes through note_launch() so the process can report
+// how many library kernels ran.
+extern std::atomic<uint64_t> g_launch_count;
+inline void note_launch(uint64_t n = 1) { g_launch_count.fetch_add(n); }
+
+// ---- device buffers ----------------------------------------------------------
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  drb_status alloc(size_t nbytes);
+  drb_status ensure(size_t nbytes); // grow (contents not kept)
+  void release();
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+constexpr int64_t kPadElems = 64;
+
+// ---- execution plan --------------------------------------------------------
+// A CTA work item ("row block").  {a, b}:
+//   b >  0 : rows [a, b), whose aligned nnz span fits one tile;
+//   b == -1: the single long row a (span > tile), one CTA loops over it;
+//   b <= -2: chunk (-b - 2) of a row too long for one CTA (see Chunk).
+struct Chunk {
+  int64_t p0, p1;   // nnz range of this chunk
+  int32_t row;      // the row it belongs to
+  int32_t first;    // first chunk index of that row
+  int32_t count;    // number of chunks of that row
+  int32_t counter;  // index of the row's completion counter
+};
+
+struct Plan {
+  int tile = 0;        // nnz capacity of a tile (aligned span)
+  int rows_max = 0;    // max rows in one tile
+  int long_max = 0;    // rows longer than this are chunked
+  int group = 0;       // elements per 16-byte vector group (G)
+  int64_t nblocks = 0; // CTA work items
+  int64_t nchunks = 0;
+  int64_t nsplit = 0;  // rows that are chunked
+  DevBuf blocks;       // int2[nblocks]
+  DevBuf chunks;       // Chunk[nchunks]
+  DevBuf partials;     // double[nchunks * kmax] (grown on demand)
+  DevBuf counters;     // int[nsplit], zero between launches
+  int64_t partial_k = 0;
+  DevBuf red;          // double[nblocks] + int ticket: residual reduction
+};
+
+struct Csr {
+  int device = 0;
+  int64_t m = 0, n = 0, nnz = 0;
+  drb_dtype value_type = DRB_F32; // caller's element type
+  drb_dtype storage = DRB_F32;    // device element type
+  int cbytes = 4, rbytes = 4;     // stored index widths
+  int nseg = 1;
+  drb_partition part = DRB_PART_ROW;
+  uint32_t flags = 0;
+  DevBuf rowptr, colind, vals;
+  Plan plan;
+  std::vector<int64_t> seg_row0, seg_row1, seg_nz0, seg_nz1;
+  // adjoint plan: A^T as a CSR matrix of shape n x m (colptr, rowidx, values
+  // in column order, its own row-block plan) and perm[nnz] (CSC position ->
+  // CSR position, perm_bytes wide) used to refresh the transposed values.
+  bool has_adjoint = false;
+  std::unique_ptr<Csr> tr;
+  DevBuf perm;
+  int perm_bytes = 4;
+  // scratch for multi-RHS layout changes and host staging
+  DevBuf xs, ys, xh_dev, yh_dev;
+  // host copy of rowptr (int64), filled on first drb_csr_get_entries
+  std::vector<int64_t> rowptr_h;
+  ~Csr();
+};
+
+// ---- launchers (defined in the .cu files) ------------------------------------
+drb_status build_plan(Plan &plan, int64_t m, const void *rowptr_host,
+                      int rbytes, int group, int tile, int rows_max,
+                      int long_max);
+
+drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
+                       drb_layout layout, cudaStream_t s);
+drb_status spmv_t_launch(Csr &A, const void *ybar, void *xbar, cudaStream_t s);
+drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
+                       cudaStream_t s);
+drb_status residual_launch(Csr &A, const void *x, const void *b, void *y,
+                           double *out, cudaStream_t s);
+drb_status adjoint_build(Csr &A, cudaStream_t s);
+drb_status adjoint_refresh_values(Csr &A, cudaStream_t s);
+drb_status dense_launch(int64_t m, int64_t n, const void *A, int64_t lda,
+                        const void *x, void *y, int64_t k, drb_layout layout,
+                        drb_dtype dt, cudaStream_t s);
+drb_status dot_launch(int64_t n, const void *a, const void *b, drb_dtype dt,
+                      double *out, cudaStream_t s);
+drb_status convert_launch(const void *in, int in_bytes, void *out,
+                          int out_bytes, int64_t count, bool to_bf16,
+                          cudaStream_t s);
+drb_status transpose_launch(const void *in, void *out, int64_t rows,
+                            int64_t cols, int elem_bytes, cudaStream_t s);
+
+inline int dtype_bytes(drb_dtype t) {
+  return t == DRB_F64 ? 8 : (t == DRB_BF16 ? 2 : 4);
+}
+
+} // namespace drb
+
+// ---- PTX helpers ---------------------------------------------------------------
+namespace drb::ptx {
+
+// L2 policies: streamed matrix data is evicted first, the gathered vector x
+// is kept (evict_last) so it stays L2-resident across the whole launch.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// 16-byte streaming load through the non-coherent path, not allocated in L1.
+__device__ __forceinline__ uint4 ld_stream16(const void *ptr, uint64_t pol) {
+  uint4 r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 "
+               "{%0,%1,%2,%3}, [%4], %5;"
+               : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+               : "l"(ptr), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ float ld_keep(const float *ptr, uint64_t pol) {
+  float r;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;"
+               : "=f"(r)
+               : "l"(ptr), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ double ld_keep(const double *ptr, uint64_t pol) {
+  double r;
+  asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;"
+               : "=d"(r)
+               : "l"(ptr), "l"(pol));
+  return r;
+}
+__device__ __forceinline__ float ld_keep(const __nv_bfloat16 *ptr,
+                                         uint64_t pol) {
+  unsigned short r;
+  asm("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;"
+               : "=h"(r)
+               : "l"(ptr), "l"(pol));
+  return __uint_as_float(((unsigned)r) << 16);
+}
+
+} // namespace drb::ptx

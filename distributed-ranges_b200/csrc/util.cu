@@ -1,0 +1,108 @@
+// util.cu -- small device kernels: layout transposes and element conversions
+// used at upload time and around multi-RHS calls.
+#include "drb_internal.cuh"
+
+namespace drb {
+namespace {
+
+// out[c][r] = in[r][c] for a rows x cols row-major input, 32x32 smem tiles.
+template <class T>
+__global__ void transpose_kernel(const T *__restrict__ in, T *__restrict__ out,
+                                 int64_t rows, int64_t cols) {
+  __shared__ T tile[32][33];
+  const int64_t c0 = (int64_t)blockIdx.x * 32, r0 = (int64_t)blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t r = r0 + i, c = c0 + threadIdx.x;
+    if (r < rows && c < cols)
+      tile[i][threadIdx.x] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t c = c0 + i, r = r0 + threadIdx.x;
+    if (r < rows && c < cols)
+      out[c * rows + r] = tile[threadIdx.x][i];
+  }
+}
+
+template <class In, class Out>
+__global__ void convert_kernel(const In *__restrict__ in, Out *__restrict__ out,
+                               int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (Out)in[i];
+}
+
+__global__ void f32_to_bf16_kernel(const float *__restrict__ in,
+                                   __nv_bfloat16 *__restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn(in[i]);
+}
+
+unsigned grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g > 148 * 32)
+    g = 148 * 32;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+} // namespace
+
+drb_status transpose_launch(const void *in, void *out, int64_t rows,
+                            int64_t cols, int elem_bytes, cudaStream_t s) {
+  if (rows == 0 || cols == 0)
+    return DRB_OK;
+  const int64_t gx = (cols + 31) / 32, gy = (rows + 31) / 32;
+  if (gy > 65535) {
+    set_error("transpose: %lld rows exceed the grid limit", (long long)rows);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  dim3 grid((unsigned)gx, (unsigned)gy), block(32, 8);
+  if (elem_bytes == 4)
+    transpose_kernel<float><<<grid, block, 0, s>>>((const float *)in,
+                                                   (float *)out, rows, cols);
+  else if (elem_bytes == 8)
+    transpose_kernel<double><<<grid, block, 0, s>>>((const double *)in,
+                                                    (double *)out, rows, cols);
+  else if (elem_bytes == 2)
+    transpose_kernel<unsigned short><<<grid, block, 0, s>>>(
+        (const unsigned short *)in, (unsigned short *)out, rows, cols);
+  else {
+    set_error("transpose: element size %d", elem_bytes);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  note_launch();
+  DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
+}
+
+// Element conversion on the device.  in_bytes/out_bytes select the types:
+//   8 -> 4 : int64 -> int32 (index narrowing; the host validated the range)
+//   4 -> 8 : int32 -> int64
+//   4 -> 2 with to_bf16 : float -> bfloat16 (round to nearest even)
+drb_status convert_launch(const void *in, int in_bytes, void *out,
+                          int out_bytes, int64_t count, bool to_bf16,
+                          cudaStream_t s) {
+  if (count == 0)
+    return DRB_OK;
+  const int T = 256;
+  const unsigned g = grid_for(count, T);
+  if (to_bf16 && in_bytes == 4 && out_bytes == 2)
+    f32_to_bf16_kernel<<<g, T, 0, s>>>((const float *)in, (__nv_bfloat16 *)out,
+                                       count);
+  else if (!to_bf16 && in_bytes == 8 && out_bytes == 4)
+    convert_kernel<int64_t, int32_t><<<g, T, 0, s>>>((const int64_t *)in,
+                                                     (int32_t *)out, count);
+  else if (!to_bf16 && in_bytes == 4 && out_bytes == 8)
+    convert_kernel<int32_t, int64_t><<<g, T, 0, s>>>((const int32_t *)in,
+                                                     (int64_t *)out, count);
+  else {
+    set_error("convert: unsupported %d -> %d", in_bytes, out_bytes);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  note_launch();
+  DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
+}
+
+} // namespace drb

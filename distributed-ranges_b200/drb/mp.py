@@ -1,0 +1,466 @@
+"""Python mirror of the reference's ``dr::mp`` gemv interface over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference
+(include/dr/mp/algorithms/matrix/gemv.hpp,
+include/dr/mp/containers/distributed_sparse_matrix.hpp,
+include/dr/mp/containers/broadcasted_vector.hpp,
+include/dr/mp/containers/broadcasted_slim_matrix.hpp,
+include/dr/views/csr_matrix_view.hpp) so a test written against the
+reference reads the same here.  One process owns one GPU: the "ranks" of the
+reference become logical segments of one device-resident matrix, rank 0 is the
+only root, and ``gemv`` runs the sm_100a kernels of libdrb.so.  Device memory
+and streams are torch's (torch.cuda tensors, the current stream).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterator, Sequence
+
+import numpy as np
+import torch
+
+from . import _capi as capi
+from ._capi import check
+
+__all__ = [
+    "csr_matrix_view", "distribution", "csr_row_distribution",
+    "csr_eq_distribution", "distributed_sparse_matrix", "broadcasted_vector",
+    "broadcasted_slim_matrix", "gemv", "gemv_backward", "dense_gemv", "dot",
+    "residual_norm2", "default_comm", "init", "finalize",
+]
+
+_TORCH_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
+             torch.bfloat16: capi.DRB_BF16}
+_NP_DT = {np.dtype(np.float32): capi.DRB_F32, np.dtype(np.float64): capi.DRB_F64}
+_NP_IT = {np.dtype(np.int32): capi.DRB_I32, np.dtype(np.int64): capi.DRB_I64,
+          np.dtype(np.uint64): capi.DRB_I64}
+_STORAGE_TORCH = {capi.DRB_F32: torch.float32, capi.DRB_F64: torch.float64,
+                  capi.DRB_BF16: torch.bfloat16}
+
+
+def _stream(stream=None) -> C.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t) -> C.c_void_p:
+    if t is None:
+        return C.c_void_p(0)
+    if isinstance(t, torch.Tensor):
+        return C.c_void_p(t.data_ptr())
+    return C.c_void_p(t.ctypes.data)
+
+
+class _Comm:
+    """The single-process communicator: rank 0 of 1 (the reference's
+    default_comm(), include/dr/mp/global.hpp)."""
+
+    def rank(self) -> int:
+        return 0
+
+    def size(self) -> int:
+        return 1
+
+
+_COMM = _Comm()
+
+
+def default_comm() -> _Comm:
+    return _COMM
+
+
+def init(device: int | None = None) -> None:
+    """mp::init(): select the CUDA device (global.hpp:130-135, 191-197)."""
+    if device is not None:
+        torch.cuda.set_device(device)
+
+
+def finalize() -> None:
+    torch.cuda.synchronize()
+
+
+class csr_matrix_view:
+    """Non-owning host CSR triple (csr_matrix_view.hpp:125-220):
+    values[nnz], rowptr[m+1], colind[nnz], shape (m, n)."""
+
+    def __init__(self, values, rowptr, colind, shape, nnz=None, rank=0):
+        self._values = np.ascontiguousarray(values)
+        self._rowptr = np.ascontiguousarray(rowptr)
+        self._colind = np.ascontiguousarray(colind)
+        self._shape = (int(shape[0]), int(shape[1]))
+        self._nnz = int(self._rowptr[self._shape[0]]) if nnz is None else int(nnz)
+        self._rank = rank
+
+    def shape(self):
+        return self._shape
+
+    def size(self) -> int:
+        return self._nnz
+
+    def rank(self) -> int:
+        return self._rank
+
+    def values_data(self):
+        return self._values
+
+    def rowptr_data(self):
+        return self._rowptr
+
+    def colind_data(self):
+        return self._colind
+
+    def __iter__(self):
+        rp, ci, v = self._rowptr, self._colind, self._values
+        for i in range(self._shape[0]):
+            for p in range(int(rp[i]), int(rp[i + 1])):
+                yield (i, int(ci[p])), v[p]
+
+
+class distribution:
+    """Distribution options (include/dr/mp/containers/distribution.hpp:11-44).
+    distributed_sparse_matrix only stores it, as the reference does."""
+
+    def __init__(self, halo=(0, 0), periodic=False, granularity=1):
+        self.halo = halo
+        self.periodic = periodic
+        self.granularity = granularity
+
+
+class csr_row_distribution:
+    """Row-block policy: segment r owns rows [r*ceil(m/P), ...)
+    (matrix_formats/csr_row_distribution.hpp)."""
+    partition = capi.DRB_PART_ROW
+
+
+class csr_eq_distribution:
+    """Equal-nnz policy, the reference's default MatrixDistrT
+    (matrix_formats/csr_eq_distribution.hpp)."""
+    partition = capi.DRB_PART_EQ
+
+
+class _Segment:
+    """One row-block segment (the reference's csr_row_segment /
+    csr_eq_segment): rank(), size(), is_local(), iteration over entries."""
+
+    def __init__(self, mat: "distributed_sparse_matrix", idx: int):
+        self._m = mat
+        self._idx = idx
+        r0, r1, z0, z1 = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64())
+        check(capi.lib.drb_csr_segment(mat._h, idx, C.byref(r0), C.byref(r1),
+                                       C.byref(z0), C.byref(z1)))
+        self.row_begin, self.row_end = r0.value, r1.value
+        self.nnz_begin, self.nnz_end = z0.value, z1.value
+
+    def rank(self) -> int:
+        return self._idx
+
+    def size(self) -> int:
+        return self.nnz_end - self.nnz_begin
+
+    def __len__(self) -> int:
+        return self.size()
+
+    def is_local(self) -> bool:
+        return True  # every segment lives on this process's GPU
+
+    def entries(self):
+        return self._m._entries(self.nnz_begin, self.size())
+
+    def __iter__(self):
+        rows, cols, vals = self.entries()
+        for i in range(len(rows)):
+            yield (int(rows[i]), int(cols[i])), vals[i]
+
+
+class distributed_sparse_matrix:
+    """distributed_sparse_matrix<T, I, Backend, MatrixDistrT>
+    (distributed_sparse_matrix.hpp:29-162) resident on one GPU.
+
+    csr_view   host csr_matrix_view (or any object with the same accessors)
+    root       the rank that holds csr_view (only 0 exists)
+    dist       distribution (stored only)
+    distr      csr_eq_distribution (default, as in the reference) or
+               csr_row_distribution
+    nsegments  number of logical segments (the reference's rank count)
+    storage    torch.bfloat16 to store f32 values as bf16
+    adjoint    build the CSC plan used by gemv_backward
+    """
+
+    def __init__(self, csr_view, root: int = 0, dist: distribution | None = None,
+                 *, distr=csr_eq_distribution, nsegments: int = 1,
+                 storage=None, adjoint: bool = False,
+                 keep_index64: bool = False, stream=None):
+        if root != 0:
+            raise ValueError(f"root {root} is not a rank: one process owns the GPU")
+        self._h = C.c_void_p(0)
+        self.distribution = dist or distribution()
+        values = np.ascontiguousarray(csr_view.values_data())
+        rowptr = np.ascontiguousarray(csr_view.rowptr_data())
+        colind = np.ascontiguousarray(csr_view.colind_data())
+        m, n = csr_view.shape()
+        nnz = int(csr_view.size())
+        if values.dtype not in _NP_DT:
+            raise TypeError(f"values dtype {values.dtype} (need float32/float64)")
+        vt = _NP_DT[values.dtype]
+        it = np.promote_types(rowptr.dtype, colind.dtype)
+        if it not in _NP_IT:
+            raise TypeError(f"index dtype {it} (need int32/int64)")
+        if rowptr.dtype != it:
+            rowptr = rowptr.astype(it)
+        if colind.dtype != it:
+            colind = colind.astype(it)
+        st = vt if storage is None else _TORCH_DT[storage]
+        flags = 0
+        if adjoint:
+            flags |= capi.DRB_FLAG_ADJOINT
+        if keep_index64:
+            flags |= capi.DRB_FLAG_KEEP_INDEX64
+        h = C.c_void_p()
+        check(capi.lib.drb_csr_create(
+            C.byref(h), m, n, nnz, _ptr(rowptr), _ptr(colind), _ptr(values),
+            _NP_IT[it], vt, st, int(nsegments), distr.partition, flags,
+            _stream(stream)))
+        self._h = h
+        self._shape = (int(m), int(n))
+        self._nnz = nnz
+        self.value_dtype = _STORAGE_TORCH[vt]
+        self.storage_dtype = _STORAGE_TORCH[st]
+        self.compute_dtype = torch.float32 if st == capi.DRB_BF16 else self.storage_dtype
+        self._ybuf: dict = {}
+
+    # ---- reference accessors ----
+    def shape(self):
+        return self._shape
+
+    def size(self) -> int:
+        return self._nnz
+
+    def nnz(self) -> int:
+        return self._nnz
+
+    def segments(self) -> list:
+        nseg = C.c_int()
+        check(capi.lib.drb_csr_num_segments(self._h, C.byref(nseg)))
+        return [_Segment(self, i) for i in range(nseg.value)]
+
+    def fence(self) -> None:
+        torch.cuda.current_stream().synchronize()
+
+    def storage_bytes(self):
+        v, c, r = C.c_int(), C.c_int(), C.c_int()
+        check(capi.lib.drb_csr_storage(self._h, C.byref(v), C.byref(c), C.byref(r)))
+        return v.value, c.value, r.value
+
+    def _entries(self, offset: int, count: int):
+        rows = np.empty(count, np.int64)
+        cols = np.empty(count, np.int64)
+        vals = np.empty(count, np.float64)
+        check(capi.lib.drb_csr_get_entries(self._h, offset, count, _ptr(rows),
+                                           _ptr(cols), _ptr(vals)))
+        return rows, cols, vals
+
+    def __iter__(self) -> Iterator:
+        rows, cols, vals = self._entries(0, self._nnz)
+        for i in range(self._nnz):
+            yield (int(rows[i]), int(cols[i])), vals[i]
+
+    def __getitem__(self, n: int):
+        rows, cols, vals = self._entries(int(n), 1)
+        return (int(rows[0]), int(cols[0])), vals[0]
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # ---- the hot call ----
+    def local_gemv_and_collect(self, root: int, res, x: torch.Tensor,
+                               width: int, stream=None) -> None:
+        """distributed_sparse_matrix.hpp:153-158: y = A x for `width` RHS
+        (column-major), result written into `res` on root."""
+        m = self._shape[0]
+        if isinstance(res, torch.Tensor) and res.is_cuda:
+            y = res
+        else:
+            key = (width,)
+            y = self._ybuf.get(key)
+            if y is None:
+                y = torch.empty(m * width, dtype=self.compute_dtype, device="cuda")
+                self._ybuf[key] = y
+        check(capi.lib.drb_csr_gemv(self._h, _ptr(x), _ptr(y), int(width),
+                                    capi.DRB_COL_MAJOR, _stream(stream)))
+        if y is res:
+            return
+        host = y.cpu().numpy()
+        if isinstance(res, np.ndarray):
+            res[...] = host.reshape(res.shape)
+        elif isinstance(res, torch.Tensor):
+            res.copy_(torch.from_numpy(host).view(res.shape))
+        else:
+            res[:] = host.tolist()
+
+    def gemv_device(self, x: torch.Tensor, y: torch.Tensor, k: int = 1,
+                    layout: int = capi.DRB_COL_MAJOR, stream=None) -> None:
+        check(capi.lib.drb_csr_gemv(self._h, _ptr(x), _ptr(y), int(k), layout,
+                                    _stream(stream)))
+
+    def gemv_host(self, x_host, y_host, k: int = 1,
+                  layout: int = capi.DRB_COL_MAJOR, stream=None) -> None:
+        check(capi.lib.drb_csr_gemv_host(self._h, _ptr(x_host), _ptr(y_host),
+                                         int(k), layout, _stream(stream)))
+
+    def update_values(self, values: torch.Tensor, stream=None) -> None:
+        check(capi.lib.drb_csr_update_values(self._h, _ptr(values), _stream(stream)))
+
+    def destroy(self) -> None:
+        if self._h and self._h.value:
+            capi.lib.drb_csr_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+
+class broadcasted_vector:
+    """x replicated on every rank (broadcasted_vector.hpp:9-51); here the
+    single copy lives on the GPU."""
+
+    def __init__(self):
+        self._data = None
+
+    def broadcast_data(self, data_size: int, root: int, root_data,
+                       comm=None, dtype=None) -> None:
+        if root != 0:
+            raise ValueError(f"root {root} is not a rank")
+        t = torch.as_tensor(np.asarray(root_data) if not isinstance(root_data, torch.Tensor) else root_data)
+        if dtype is not None:
+            t = t.to(dtype)
+        t = t.reshape(-1)[:data_size].contiguous()
+        if t.numel() != data_size:
+            raise ValueError("root_data shorter than data_size")
+        self._data = t.cuda()
+
+    def destroy_data(self) -> None:
+        self._data = None
+
+    def broadcasted_data(self) -> torch.Tensor:
+        return self._data
+
+    def size(self) -> int:
+        return 0 if self._data is None else self._data.numel()
+
+    def __getitem__(self, i):
+        return self._data[i]
+
+
+class broadcasted_slim_matrix:
+    """A height x width block replicated on every rank, column-major:
+    element (i, j) at i + j*height (broadcasted_slim_matrix.hpp:9-80)."""
+
+    def __init__(self):
+        self._data = None
+        self._width = 0
+        self._height = 0
+
+    def broadcast_data(self, height: int, width: int, root: int, root_data,
+                       comm=None, dtype=None) -> None:
+        if root != 0:
+            raise ValueError(f"root {root} is not a rank")
+        if isinstance(root_data, (list, tuple)) and root_data and hasattr(root_data[0], "__len__") \
+                and len(root_data) == width and not isinstance(root_data[0], (int, float)):
+            cols = [np.asarray(c)[:height] for c in root_data]  # T** overload
+            arr = np.concatenate(cols)
+        else:
+            arr = np.asarray(root_data).reshape(-1)[: height * width]
+        t = torch.as_tensor(arr)
+        if dtype is not None:
+            t = t.to(dtype)
+        self._data = t.contiguous().cuda()
+        self._width = width
+        self._height = height
+
+    def destroy_data(self) -> None:
+        self._data = None
+
+    def broadcasted_data(self) -> torch.Tensor:
+        return self._data
+
+    def width(self) -> int:
+        return self._width
+
+    def __getitem__(self, j):
+        return self._data[j * self._height:(j + 1) * self._height]
+
+
+def gemv(*args, stream=None) -> None:
+    """dr::mp::gemv overloads (gemv.hpp:16-71):
+        gemv(root, res, A, b)  -> result on root
+        gemv(res, A, b)        -> result everywhere (one rank here)
+    b is a broadcasted_vector or broadcasted_slim_matrix; res holds
+    m (or m*width, column-major) elements."""
+    if len(args) == 4:
+        root, res, a, b = args
+    elif len(args) == 3:
+        res, a, b = args
+        root = 0
+    else:
+        raise TypeError("gemv(root, res, A, b) or gemv(res, A, b)")
+    m, n = a.shape()
+    if isinstance(b, broadcasted_slim_matrix):
+        width = b.width()
+        if m * width != len(res):
+            raise ValueError(f"res has {len(res)} elements, expected {m * width}")
+    else:
+        width = 1
+        if m != len(res):
+            raise ValueError(f"res has {len(res)} elements, expected {m}")
+        if b.size() != n:
+            raise ValueError(f"x has {b.size()} elements, expected {n}")
+    x = b.broadcasted_data()
+    if x.dtype != a.compute_dtype and not (a.storage_dtype == torch.bfloat16 and x.dtype == torch.bfloat16):
+        x = x.to(a.storage_dtype)
+    a.local_gemv_and_collect(root, res, x, width, stream=stream)
+
+
+def gemv_backward(a: distributed_sparse_matrix, ybar: torch.Tensor,
+                  x: torch.Tensor | None = None, xbar: torch.Tensor | None = None,
+                  abar: torch.Tensor | None = None, stream=None) -> None:
+    """Adjoint of y = A x: xbar = A^T ybar, abar[p] = ybar[row p] * x[col p]."""
+    check(capi.lib.drb_csr_gemv_backward(a.handle, _ptr(ybar), _ptr(x), _ptr(xbar),
+                                         _ptr(abar), _stream(stream)))
+
+
+def residual_norm2(a: distributed_sparse_matrix, x: torch.Tensor, b: torch.Tensor,
+                   y: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """|| A x - b ||^2 fused into the SpMV epilogue (f64 device scalar)."""
+    out = torch.empty(1, dtype=torch.float64, device="cuda")
+    check(capi.lib.drb_csr_residual_norm2(a.handle, _ptr(x), _ptr(b), _ptr(y),
+                                          _ptr(out), _stream(stream)))
+    return out
+
+
+def dense_gemv(A: torch.Tensor, x: torch.Tensor, y: torch.Tensor, k: int = 1,
+               layout: int = capi.DRB_COL_MAJOR, stream=None) -> None:
+    """y = A x for a row-major (m, n) tensor A with k RHS."""
+    m, n = A.shape
+    lda = A.stride(0)
+    check(capi.lib.drb_dense_gemv(m, n, _ptr(A), lda, _ptr(x), _ptr(y), int(k), layout,
+                                  _TORCH_DT[A.dtype], _stream(stream)))
+
+
+def dot(a: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None,
+        stream=None) -> torch.Tensor:
+    """sum(a*b) in f64 with a fixed order (a is b: squared norm)."""
+    if out is None:
+        out = torch.empty(1, dtype=torch.float64, device="cuda")
+    check(capi.lib.drb_dot(a.numel(), _ptr(a), _ptr(b), _TORCH_DT[a.dtype], _ptr(out),
+                           _stream(stream)))
+    return out

@@ -1,0 +1,179 @@
+/*
+ * drb.h -- C ABI of the B200-native gemv hot path of Distributed Ranges.
+ *
+ * One process owns one B200.  A CSR matrix is uploaded once into a handle
+ * (device-resident row-block segments plus the execution plan) and multiplied
+ * many times, as dr::mp::distributed_sparse_matrix is constructed once and
+ * passed to dr::mp::gemv repeatedly.  Every entry point is extern "C", takes
+ * plain pointers and sizes, never throws, and returns a drb_status.  After a
+ * non-zero status, drb_last_error() returns a message for the calling thread.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   drb_csr_create / drb_csr_destroy
+ *       distributed_sparse_matrix(csr_matrix_view, root, distribution)
+ *       include/dr/mp/containers/distributed_sparse_matrix.hpp:131-134, with
+ *       csr_row_distribution::init (matrix_formats/csr_row_distribution.hpp:
+ *       205-318) or csr_eq_distribution::init (csr_eq_distribution.hpp:
+ *       220-333) and the destructors (:33-42 / :33-41).
+ *   drb_csr_shape / drb_csr_num_segments / drb_csr_segment /
+ *   drb_csr_get_entries
+ *       shape(), nnz(), segments() and the segment iterator's get()
+ *       (distributed_sparse_matrix.hpp:141-149; csr_row_segment.hpp:140-208).
+ *   drb_csr_gemv / drb_csr_gemv_host
+ *       dr::mp::gemv(root, res, A, broadcasted_vector | broadcasted_slim_matrix)
+ *       include/dr/mp/algorithms/matrix/gemv.hpp:16-39 ->
+ *       local_gemv_and_collect (distributed_sparse_matrix.hpp:153-158,
+ *       csr_row_distribution.hpp:137-153, csr_eq_distribution.hpp:134-153).
+ *
+ * Entry points with no reference counterpart (new API shaped after gemv):
+ *   drb_dense_gemv, drb_dot, drb_csr_residual_norm2, drb_csr_gemv_backward,
+ *   drb_csr_update_values, drb_batch_*.
+ *
+ * Layouts.  Multi-RHS blocks follow broadcasted_slim_matrix: column-major,
+ * x[c + j*n], y[r + j*m] (gemv.hpp:29-39, csr_row_distribution.hpp:129-130).
+ * DRB_ROW_MAJOR (x[c*k + j], y[r*k + j]) is also accepted.
+ *
+ * Threads and streams.  Distinct handles may be used concurrently on distinct
+ * streams; one handle must not be used by two threads at once.  All compute
+ * entry points are asynchronous on the given stream (a cudaStream_t passed as
+ * void*; NULL = the legacy default stream) except the *_host variants, which
+ * synchronise the stream before returning.
+ */
+#ifndef DRB_H
+#define DRB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int drb_status;
+#define DRB_OK 0
+#define DRB_ERR_INVALID_ARG 1 /* null pointer, negative size, bad enum      */
+#define DRB_ERR_BAD_CSR 2     /* rowptr not monotone / column out of range  */
+#define DRB_ERR_OOM 3         /* device or pinned host allocation failed    */
+#define DRB_ERR_CUDA 4        /* a CUDA runtime call failed                 */
+#define DRB_ERR_TIMEOUT 5     /* a bounded device-side wait expired         */
+#define DRB_ERR_UNSUPPORTED 6 /* valid request this build does not handle   */
+#define DRB_ERR_NO_DEVICE 7   /* no CUDA device / wrong architecture        */
+
+typedef enum { DRB_F32 = 0, DRB_F64 = 1, DRB_BF16 = 2 } drb_dtype;
+typedef enum { DRB_I32 = 0, DRB_I64 = 1 } drb_itype;
+typedef enum { DRB_COL_MAJOR = 0, DRB_ROW_MAJOR = 1 } drb_layout;
+/* How the rows are split into segments (the reference's MatrixDistrT):
+ * DRB_PART_ROW = csr_row_distribution (rank r owns rows [r*ceil(m/P), ...)),
+ * DRB_PART_EQ  = csr_eq_distribution (rank r owns nnz [r*ceil(nnz/P), ...);
+ *                a row that straddles two segments is summed from both). */
+typedef enum { DRB_PART_ROW = 0, DRB_PART_EQ = 1 } drb_partition;
+
+/* drb_csr_create flags */
+#define DRB_FLAG_DEVICE_INPUT 0x1u   /* rowptr/colind/values are device ptrs */
+#define DRB_FLAG_KEEP_INDEX64 0x2u   /* keep 64-bit indices on the device    */
+#define DRB_FLAG_SKIP_VALIDATE 0x4u  /* skip the host-side CSR validation    */
+#define DRB_FLAG_ADJOINT 0x8u        /* build the CSC plan for gemv_backward */
+#define DRB_FLAG_COMPENSATED 0x10u   /* two-sum compensated FP32 row sums    */
+
+typedef struct drb_csr_matrix *drb_csr_t;
+
+/* ---- lifecycle ------------------------------------------------------------ */
+
+/* Upload an m x n CSR matrix (rowptr[m+1], colind[nnz], values[nnz]; the
+ * csr_matrix_view triple, csr_matrix_view.hpp:125-220) and build its plan.
+ * value_type is the caller's element type (F32 or F64); storage is the device
+ * element type: equal to value_type, or DRB_BF16 for F32 input (values are
+ * rounded to bfloat16, gemv then takes bf16 x and writes f32 y).  nsegments
+ * is the number of logical segments (the reference's MPI rank count; >= 1);
+ * all segments live on the current device.  Index width: 64-bit input
+ * indices are narrowed to 32 bits on the device when they fit, unless
+ * DRB_FLAG_KEEP_INDEX64.  The stream orders the uploads; the call returns
+ * after they complete. */
+drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
+                          const void *rowptr, const void *colind,
+                          const void *values, drb_itype index_type,
+                          drb_dtype value_type, drb_dtype storage,
+                          int nsegments, drb_partition partition,
+                          uint32_t flags, void *stream);
+
+drb_status drb_csr_destroy(drb_csr_t A);
+
+drb_status drb_csr_shape(drb_csr_t A, int64_t *m, int64_t *n, int64_t *nnz);
+
+/* Device storage actually used: value bytes, column-index bytes, rowptr
+ * bytes per element (for algorithmic-byte accounting). */
+drb_status drb_csr_storage(drb_csr_t A, int *value_bytes, int *col_bytes,
+                           int *rowptr_bytes);
+
+drb_status drb_csr_num_segments(drb_csr_t A, int *nsegments);
+
+/* Row and nnz range of segment `seg` (csr_row: rows [r*ceil(m/P), ...) and
+ * their nnz; csr_eq: nnz [r*ceil(nnz/P), ...) and the rows they touch). */
+drb_status drb_csr_segment(drb_csr_t A, int seg, int64_t *row_begin,
+                           int64_t *row_end, int64_t *nnz_begin,
+                           int64_t *nnz_end);
+
+/* Copy `count` entries starting at global nnz offset `offset` to host arrays
+ * (row, column, value as double); any output pointer may be NULL.  This is
+ * the global iterator's dereference (distributed_sparse_matrix.hpp:103-107). */
+drb_status drb_csr_get_entries(drb_csr_t A, int64_t offset, int64_t count,
+                               int64_t *rows, int64_t *cols, double *values);
+
+/* ---- the hot call ------------------------------------------------------- */
+
+/* y = A * x for k right-hand sides, device pointers.  Element types: x and y
+ * have the storage type, except BF16 storage: x bf16, y f32.  y is
+ * overwritten (the reference zero-fills its partial result first). */
+drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
+                        drb_layout layout, void *stream);
+
+/* Same product with HOST x and y (any host memory; pinned is fastest): the
+ * call copies x to the device, multiplies, copies y back and synchronises,
+ * as gemv(root, res, A, x) returns res on the host. */
+drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
+                             int64_t k, drb_layout layout, void *stream);
+
+/* Fused residual: out[0] = || A*x - b ||_2^2 accumulated in f64 (device
+ * double*), y = A*x also written when y != NULL.  k = 1. */
+drb_status drb_csr_residual_norm2(drb_csr_t A, const void *x, const void *b,
+                                  void *y, double *out, void *stream);
+
+/* ---- adjoint (needs DRB_FLAG_ADJOINT at create) ------------------------- */
+
+/* For L(y) with y = A x and upstream gradient ybar (length m):
+ *   xbar = A^T ybar (length n), atomics-free over the CSC plan;
+ *   abar[p] = ybar[row(p)] * x[col(p)] for every stored entry p (CSR order).
+ * Either output may be NULL to skip it.  Types as drb_csr_gemv (k = 1). */
+drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
+                                 void *xbar, void *abar, void *stream);
+
+/* Replace the stored values (device pointer, CSR order, storage type) and
+ * refresh the CSC copy used by gemv_backward. */
+drb_status drb_csr_update_values(drb_csr_t A, const void *values,
+                                 void *stream);
+
+/* ---- dense and reductions ------------------------------------------------ */
+
+/* y = A x for a row-major m x n matrix (leading dimension lda >= n), k RHS in
+ * `layout`.  F32 or F64 (accumulated in the element type).  Device ptrs. */
+drb_status drb_dense_gemv(int64_t m, int64_t n, const void *A, int64_t lda,
+                          const void *x, void *y, int64_t k, drb_layout layout,
+                          drb_dtype dtype, void *stream);
+
+/* out[0] = sum_i a[i]*b[i] (a == b gives the squared norm), f64 accumulation
+ * with a deterministic order; out is a device double*.  F32 or F64. */
+drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
+                   double *out, void *stream);
+
+/* ---- misc ----------------------------------------------------------------- */
+
+const char *drb_last_error(void);
+const char *drb_version(void);
+/* Number of kernels this library has launched in the calling process. */
+uint64_t drb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRB_H */

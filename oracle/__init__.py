@@ -1,0 +1,199 @@
+"""Python access to the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, always as the checker or the timed CPU
+baseline, never as the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_GEN = os.path.join(HERE, "_ref", "ref_gen")
+
+F32, F64 = 0, 1
+I32, I64, U64 = 0, 1, 2
+ACC_T, ACC_F64, ACC_LD = 0, 1, 2
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"oracle not built ({LIB_PATH}); run make -C oracle")
+
+lib = C.CDLL(LIB_PATH)
+_v, _i64, _i = C.c_void_p, C.c_int64, C.c_int
+_SIGS = {
+    "orc_random_csr_nnz": (_i64, [_i64, _i64, C.c_double]),
+    "orc_gen_random_csr": (_i, [_i, _i, _i64, _i64, C.c_double, C.c_uint32, _v, _v, _v]),
+    "orc_band_csr_nnz": (_i64, [_i64, _i64, _i64]),
+    "orc_gen_band_csr": (_i, [_i, _i, _i64, _i64, _i64, _v, _v, _v]),
+    "orc_csr_gemv_row": (_i, [_i, _i, _i, _i64, _i64, _v, _v, _v, _v, _i64, _v, _i]),
+    "orc_csr_gemv_eq": (_i, [_i, _i, _i, _i64, _i64, _v, _v, _v, _v, _i64, _v, _i]),
+    "orc_csr_gemv_row_threads": (_i, [_i, _i, _i64, _i64, _v, _v, _v, _v, _i64, _v, _i,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "orc_csr_absdot": (_i, [_i, _i, _i64, _i64, _v, _v, _v, _v, _i64, _v]),
+    "orc_dense_gemv": (_i, [_i, _i, _i64, _i64, _v, _i64, _v, _i64, _v]),
+    "orc_csr_transpose": (_i, [_i, _i, _i64, _i64, _v, _v, _v, _v, _v, _v]),
+    "orc_csr_abar": (_i, [_i, _i, _i64, _v, _v, _v, _v, _v]),
+    "orc_dot": (C.c_double, [_i, _i64, _v, _v]),
+    "orc_f32_to_bf16": (None, [_i64, _v, _v]),
+    "orc_bf16_to_f32": (None, [_i64, _v, _v]),
+}
+for _n, (_r, _a) in _SIGS.items():
+    _f = getattr(lib, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+
+
+def vcode(dtype) -> int:
+    return {np.dtype(np.float32): F32, np.dtype(np.float64): F64}[np.dtype(dtype)]
+
+
+def icode(dtype) -> int:
+    return {np.dtype(np.int32): I32, np.dtype(np.int64): I64,
+            np.dtype(np.uint64): U64}[np.dtype(dtype)]
+
+
+def random_csr(m, n, density, seed=0, value_dtype=np.float32, index_dtype=np.uint64):
+    """dr::generate_random_csr<T, I>(shape, density, seed), restated."""
+    nnz = lib.orc_random_csr_nnz(m, n, density)
+    rp = np.empty(m + 1, index_dtype)
+    ci = np.empty(max(nnz, 1), index_dtype)[:nnz]
+    v = np.empty(max(nnz, 1), value_dtype)[:nnz]
+    rc = lib.orc_gen_random_csr(vcode(value_dtype), icode(index_dtype), m, n, density,
+                                seed, _p(rp), _p(ci), _p(v))
+    assert rc == 0
+    return rp, ci, v
+
+
+def band_csr(size, up=3, down=3, value_dtype=np.float32, index_dtype=np.uint64):
+    """dr::generate_band_csr<T, I>(size, up, down), restated."""
+    nnz = lib.orc_band_csr_nnz(size, up, down)
+    rp = np.empty(size + 1, index_dtype)
+    ci = np.empty(nnz, index_dtype)
+    v = np.empty(nnz, value_dtype)
+    rc = lib.orc_gen_band_csr(vcode(value_dtype), icode(index_dtype), size, up, down,
+                              _p(rp), _p(ci), _p(v))
+    assert rc == 0
+    return rp, ci, v
+
+
+def _gemv(fn, rp, ci, v, x, m, n, k, acc, nseg):
+    x = np.ascontiguousarray(x, dtype=v.dtype)
+    out_dtype = v.dtype if acc == ACC_T else np.float64
+    y = np.empty(max(m * k, 1), out_dtype)[: m * k]
+    rc = fn(vcode(v.dtype), icode(ci.dtype), acc, m, n, _p(rp), _p(ci), _p(v), _p(x), k,
+            _p(y), nseg)
+    assert rc == 0, "oracle gemv failed"
+    return y
+
+
+def gemv_row(rp, ci, v, x, m, n, k=1, acc=ACC_T, nseg=1):
+    """csr_row_distribution CPU loop + gather; x, y column-major."""
+    return _gemv(lib.orc_csr_gemv_row, rp, ci, v, x, m, n, k, acc, nseg)
+
+
+def gemv_eq(rp, ci, v, x, m, n, k=1, acc=ACC_T, nseg=1):
+    """csr_eq_distribution CPU loop + split-row gather; x, y column-major."""
+    return _gemv(lib.orc_csr_gemv_eq, rp, ci, v, x, m, n, k, acc, nseg)
+
+
+def gemv_row_threads(rp, ci, v, x, m, n, k=1, nthreads=1):
+    x = np.ascontiguousarray(x, dtype=v.dtype)
+    y = np.empty(max(m * k, 1), v.dtype)[: m * k]
+    tl, tg = C.c_double(), C.c_double()
+    rc = lib.orc_csr_gemv_row_threads(vcode(v.dtype), icode(ci.dtype), m, n, _p(rp),
+                                      _p(ci), _p(v), _p(x), k, _p(y), nthreads,
+                                      C.byref(tl), C.byref(tg))
+    assert rc == 0
+    return y, tl.value, tg.value
+
+
+def absdot(rp, ci, v, x, m, n, k=1):
+    x = np.ascontiguousarray(x, dtype=v.dtype)
+    d = np.empty(max(m * k, 1), np.float64)[: m * k]
+    assert lib.orc_csr_absdot(vcode(v.dtype), icode(ci.dtype), m, n, _p(rp), _p(ci), _p(v),
+                              _p(x), k, _p(d)) == 0
+    return d
+
+
+def dense_gemv(A, x, k=1, acc=ACC_F64):
+    m, n = A.shape
+    A = np.ascontiguousarray(A)
+    x = np.ascontiguousarray(x, dtype=A.dtype)
+    y = np.empty(m * k, A.dtype if acc == ACC_T else np.float64)
+    assert lib.orc_dense_gemv(vcode(A.dtype), acc, m, n, _p(A), n, _p(x), k, _p(y)) == 0
+    return y
+
+
+def transpose(rp, ci, v, m, n):
+    nnz = int(rp[m])
+    cp = np.empty(n + 1, ci.dtype)
+    ri = np.empty(max(nnz, 1), ci.dtype)[:nnz]
+    vt = np.empty(max(nnz, 1), v.dtype)[:nnz]
+    assert lib.orc_csr_transpose(vcode(v.dtype), icode(ci.dtype), m, n, _p(rp), _p(ci),
+                                 _p(v), _p(cp), _p(ri), _p(vt)) == 0
+    return cp, ri, vt
+
+
+def abar(rp, ci, ybar, x, m):
+    nnz = int(rp[m])
+    ybar = np.ascontiguousarray(ybar)
+    x = np.ascontiguousarray(x, dtype=ybar.dtype)
+    out = np.empty(max(nnz, 1), np.float64)[:nnz]
+    assert lib.orc_csr_abar(vcode(ybar.dtype), icode(ci.dtype), m, _p(rp), _p(ci),
+                            _p(ybar), _p(x), _p(out)) == 0
+    return out
+
+
+def dot(a, b):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b, dtype=a.dtype)
+    return float(lib.orc_dot(vcode(a.dtype), a.size, _p(a), _p(b)))
+
+
+def f32_to_bf16_bits(a):
+    a = np.ascontiguousarray(a, np.float32)
+    out = np.empty(a.size, np.uint16)
+    lib.orc_f32_to_bf16(a.size, _p(a), _p(out))
+    return out
+
+
+def bf16_bits_to_f32(b):
+    b = np.ascontiguousarray(b, np.uint16)
+    out = np.empty(b.size, np.float32)
+    lib.orc_bf16_to_f32(b.size, _p(b), _p(out))
+    return out
+
+
+def fp_equal(a, b, eps=None) -> bool:
+    """The reference tests' fp_equal (test/gtest/include/common-tests.hpp:
+    82-111): |a-b| < max(min_normal, eps*(|a|+|b|)), eps = 128 * machine eps
+    of the element type; identical values always pass."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    ft = np.result_type(a.dtype, b.dtype)
+    if eps is None:
+        eps = 128 * np.finfo(ft).eps
+    tiny = np.finfo(ft).tiny
+    diff = np.abs(a.astype(np.float64) - b.astype(np.float64))
+    norm = np.minimum(np.abs(a.astype(np.float64)) + np.abs(b.astype(np.float64)),
+                      np.finfo(np.float32).max)
+    ok = (a == b) | (diff < np.maximum(tiny, eps * norm))
+    return bool(np.all(ok))
+
+
+def read_ref_bin(path):
+    """Read a CSR written by oracle/_ref/ref_gen (or a fixture in that
+    layout): int64 m, n, nnz; rowptr; colind; values."""
+    raw = open(path, "rb").read()
+    m, n, nnz = np.frombuffer(raw[:24], np.int64)
+    return int(m), int(n), int(nnz), raw[24:]

@@ -1,0 +1,523 @@
+// oracle.cpp -- CPU restatement of the Distributed Ranges gemv hot path.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA path (tests/, smoke(),
+// and bench.py's CPU-baseline leg).  The product never calls it.
+//
+// Compiled with -ffp-contract=off so every multiply and add rounds exactly as
+// the reference's scalar loop does (no fused multiply-add contraction).
+#include "oracle.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <thread>
+#include <unordered_set>
+#include <utility>
+#include <vector>
+
+namespace {
+
+struct pair_hash_u {
+  template <class I> std::size_t operator()(const std::pair<I, I> &v) const {
+    // Any hash works: membership only; entry order comes from the sort below.
+    return std::hash<unsigned long long>()((unsigned long long)v.first *
+                                               1000003ull ^
+                                           (unsigned long long)v.second);
+  }
+};
+
+template <class T> struct value_dist {
+  using type = std::uniform_real_distribution<T>;
+};
+
+// --- generate_random_csr (generate_csr.hpp:40-103) -----------------------
+template <class T, class I>
+void gen_random(int64_t m, int64_t n, double density, uint32_t seed,
+                I *rowptr, I *colind, T *vals) {
+  // generate_csr.hpp:48: nnz = size_t(density * shape[0] * shape[1]),
+  // evaluated left to right in double.
+  std::size_t nnz = (std::size_t)(density * (I)m * (I)n);
+  std::unordered_set<std::pair<I, I>, pair_hash_u> seen;
+  std::vector<std::pair<std::pair<I, I>, T>> entries;
+  entries.reserve(nnz);
+  // generate_csr.hpp:51-55: one mt19937 engine drives row, column and value.
+  std::mt19937 gen(seed);
+  std::uniform_int_distribution<I> row((I)0, (I)m - 1);
+  std::uniform_int_distribution<I> col((I)0, (I)n - 1);
+  typename value_dist<T>::type value_gen(0, 1);
+  // generate_csr.hpp:57-65: draw row, then column; a value is drawn only for
+  // a pair not seen before.
+  while (seen.size() < nnz) {
+    I i = row(gen);
+    I j = col(gen);
+    if (seen.find({i, j}) == seen.end()) {
+      T v = value_gen(gen);
+      seen.insert({i, j});
+      entries.push_back({{i, j}, v});
+    }
+  }
+  // generate_csr.hpp:74: keys are unique, so the sorted order is total.
+  std::sort(entries.begin(), entries.end());
+  // generate_csr.hpp:70-100: CSR fill with a row cursor.
+  rowptr[0] = 0;
+  std::size_t r = 0, c = 0;
+  for (auto &e : entries) {
+    I i = e.first.first;
+    vals[c] = e.second;
+    colind[c] = e.first.second;
+    while (r < (std::size_t)i) {
+      rowptr[r + 1] = (I)c;
+      r++;
+    }
+    c++;
+  }
+  for (; r < (std::size_t)m; r++)
+    rowptr[r + 1] = (I)nnz;
+}
+
+// --- generate_band_csr (generate_csr.hpp:108-153) -------------------------
+template <class T, class I>
+void gen_band(int64_t size, int64_t up, int64_t down, I *rowptr, I *colind,
+              T *vals) {
+  rowptr[0] = 0;
+  std::size_t c = 0;
+  for (int64_t i = 0; i < size; i++) {
+    for (int64_t j = std::max<int64_t>(i - down, 0); j < i; j++) {
+      vals[c] = 1;
+      colind[c] = (I)j;
+      c++;
+    }
+    vals[c] = 1;
+    colind[c] = (I)i;
+    c++;
+    for (int64_t j = i + 1; j <= i + up; j++) {
+      if (j >= size)
+        continue;
+      vals[c] = 1;
+      colind[c] = (I)j;
+      c++;
+    }
+    rowptr[i + 1] = (I)c;
+  }
+}
+
+template <class Acc, class T> struct acc_out {
+  using type = double;
+};
+template <class T> struct acc_out<T, T> {
+  using type = T;
+};
+
+// --- csr_row_distribution::local_gemv CPU branch + gather -----------------
+// csr_row_distribution.hpp:116-133 (loop), :159-204 (gather), :234-262
+// (segment nnz ranges), distributed_vector.hpp:310 (segment size ceil(m/P)).
+template <class T, class I, class Acc, class Out>
+void gemv_row_segment(int64_t m, int64_t n, const I *rowptr, const I *colind,
+                      const T *vals, const T *x, int64_t k, int64_t seg,
+                      int64_t rank, Acc *partial /* seg*k, zeroed */) {
+  if (m <= seg * rank)
+    return;
+  int64_t size = std::min(seg, m - seg * rank);
+  const I *local_rows = rowptr + seg * rank; // the rank's rowptr slice
+  int64_t first = seg * rank;
+  int64_t lower = (int64_t)rowptr[first];
+  int64_t higher =
+      (seg * (rank + 1) < m) ? (int64_t)rowptr[seg * (rank + 1)] : (int64_t)rowptr[m];
+  int64_t val_count = higher - lower;
+  int64_t row_i = 0;
+  int64_t position = lower;
+  int64_t current_row_position = size > 1 ? (int64_t)local_rows[1] : 0;
+  for (int64_t i = 0; i < val_count; i++) {
+    while (row_i + 1 < size && position + i >= current_row_position) {
+      row_i++;
+      current_row_position = (int64_t)local_rows[row_i + 1];
+    }
+    for (int64_t j = 0; j < k; j++) {
+      partial[row_i + j * seg] +=
+          (Acc)vals[lower + i] * (Acc)x[(int64_t)colind[lower + i] + j * n];
+    }
+  }
+}
+
+template <class T, class I, class Acc, class Out>
+void gemv_row(int64_t m, int64_t n, const I *rowptr, const I *colind,
+              const T *vals, const T *x, int64_t k, Out *y, int nseg) {
+  int64_t P = std::max(nseg, 1);
+  int64_t seg = (m + P - 1) / P;
+  std::vector<Acc> partial;
+  for (int64_t r = 0; r < P; r++) {
+    partial.assign((size_t)std::max<int64_t>(seg * k, 1), (Acc)0);
+    gemv_row_segment<T, I, Acc, Out>(m, n, rowptr, colind, vals, x, k, seg, r,
+                                     partial.data());
+    if (r * seg >= m)
+      break;
+    int64_t cnt = std::min(seg, m - r * seg);
+    for (int64_t j = 0; j < k; j++)
+      for (int64_t i = 0; i < cnt; i++)
+        y[m * j + r * seg + i] = (Out)partial[i + j * seg];
+  }
+}
+
+// --- csr_eq_distribution::local_gemv CPU branch + gather ------------------
+// csr_eq_distribution.hpp:112-130 (loop), :159-216 (gather with split-row
+// add), :253-272 (row ranges by upper_bound over rowptr[0..m)).
+template <class T, class I, class Acc, class Out>
+void gemv_eq(int64_t m, int64_t n, const I *rowptr, const I *colind,
+             const T *vals, const T *x, int64_t k, Out *y, int nseg) {
+  int64_t P = std::max(nseg, 1);
+  int64_t nnz = (int64_t)rowptr[m];
+  int64_t seg = (nnz + P - 1) / P; // distributed_vector<T>(nnz) segment size
+  std::vector<int64_t> row_off(P), row_sz(P);
+  for (int64_t r = 0; r < P; r++) {
+    uint64_t first_index = (uint64_t)(seg * r);
+    uint64_t last_index = (uint64_t)(seg * (r + 1)) - 1; // may wrap when seg=0
+    auto ub = [&](uint64_t v) {
+      int64_t lo = 0, hi = m; // upper_bound over rowptr[0..m)
+      while (lo < hi) {
+        int64_t mid = (lo + hi) / 2;
+        if ((uint64_t)rowptr[mid] <= v)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      return lo;
+    };
+    int64_t lower = ub(first_index) - 1;
+    int64_t higher = ub(last_index);
+    row_off[r] = lower;
+    row_sz[r] = higher - lower;
+  }
+  for (int64_t i = 0; i < m * k; i++)
+    y[i] = (Out)0; // rng::fill(res, 0) (:185)
+  std::vector<Acc> partial;
+  for (int64_t r = 0; r < P; r++) {
+    int64_t size = row_sz[r];
+    partial.assign((size_t)std::max<int64_t>(size * k, 1), (Acc)0);
+    if (!(nnz <= seg * r)) {
+      const I *rows_data = rowptr + row_off[r];
+      int64_t row_i = -1;
+      int64_t position = seg * r;
+      int64_t elem_count = std::min(seg, nnz - seg * r);
+      int64_t current_row_position = (int64_t)rows_data[0];
+      for (int64_t i = 0; i < elem_count; i++) {
+        while (row_i + 1 < size && position + i >= current_row_position) {
+          row_i++;
+          // rows_data[size] is read past the segment's rowptr slice when
+          // row_i + 1 == size; its value is never compared (the loop
+          // condition's first clause fails), so any in-bounds value is
+          // equivalent.
+          current_row_position =
+              (row_off[r] + row_i + 1 <= m) ? (int64_t)rows_data[row_i + 1] : 0;
+        }
+        for (int64_t j = 0; j < k; j++)
+          partial[row_i + j * size] += (Acc)vals[position + i] *
+                                       (Acc)x[(int64_t)colind[position + i] + j * n];
+      }
+    }
+    // gather: add the first row, copy the others (:193-202)
+    for (int64_t j = 0; j < k; j++) {
+      int64_t first_row = row_off[r], last_row = row_off[r] + size;
+      if (first_row < last_row)
+        y[first_row + j * m] = (Out)((Acc)y[first_row + j * m] + partial[j * size]);
+      for (int64_t q = 1; q < last_row - first_row; q++)
+        y[first_row + q + j * m] = (Out)partial[j * size + q];
+    }
+  }
+}
+
+template <class T, class I>
+int dispatch_acc(int acc, int eq, int64_t m, int64_t n, const void *rp,
+                 const void *ci, const void *v, const void *x, int64_t k,
+                 void *y, int nseg) {
+  auto R = (const I *)rp;
+  auto C = (const I *)ci;
+  auto V = (const T *)v;
+  auto X = (const T *)x;
+  if (acc == ORC_ACC_T) {
+    if (eq)
+      gemv_eq<T, I, T, T>(m, n, R, C, V, X, k, (T *)y, nseg);
+    else
+      gemv_row<T, I, T, T>(m, n, R, C, V, X, k, (T *)y, nseg);
+  } else if (acc == ORC_ACC_F64) {
+    if (eq)
+      gemv_eq<T, I, double, double>(m, n, R, C, V, X, k, (double *)y, nseg);
+    else
+      gemv_row<T, I, double, double>(m, n, R, C, V, X, k, (double *)y, nseg);
+  } else if (acc == ORC_ACC_LD) {
+    if (eq)
+      gemv_eq<T, I, long double, double>(m, n, R, C, V, X, k, (double *)y, nseg);
+    else
+      gemv_row<T, I, long double, double>(m, n, R, C, V, X, k, (double *)y,
+                                          nseg);
+  } else {
+    return 1;
+  }
+  return 0;
+}
+
+#define ORC_DISPATCH(vtype, itype, ...)                                       \
+  do {                                                                         \
+    if (vtype == ORC_F32 && itype == ORC_I32) {                                \
+      using T = float;                                                         \
+      using I = int32_t;                                                       \
+      __VA_ARGS__;                                                                  \
+    } else if (vtype == ORC_F32 && itype == ORC_I64) {                         \
+      using T = float;                                                         \
+      using I = int64_t;                                                       \
+      __VA_ARGS__;                                                                  \
+    } else if (vtype == ORC_F32 && itype == ORC_U64) {                         \
+      using T = float;                                                         \
+      using I = unsigned long;                                                 \
+      __VA_ARGS__;                                                                  \
+    } else if (vtype == ORC_F64 && itype == ORC_I32) {                         \
+      using T = double;                                                        \
+      using I = int32_t;                                                       \
+      __VA_ARGS__;                                                                  \
+    } else if (vtype == ORC_F64 && itype == ORC_I64) {                         \
+      using T = double;                                                        \
+      using I = int64_t;                                                       \
+      __VA_ARGS__;                                                                  \
+    } else if (vtype == ORC_F64 && itype == ORC_U64) {                         \
+      using T = double;                                                        \
+      using I = unsigned long;                                                 \
+      __VA_ARGS__;                                                                  \
+    } else {                                                                   \
+      return 1;                                                                \
+    }                                                                          \
+  } while (0)
+
+} // namespace
+
+extern "C" {
+
+int64_t orc_random_csr_nnz(int64_t m, int64_t n, double density) {
+  return (int64_t)(std::size_t)(density * (unsigned long)m * (unsigned long)n);
+}
+
+int orc_gen_random_csr(int vtype, int itype, int64_t m, int64_t n,
+                       double density, uint32_t seed, void *rowptr,
+                       void *colind, void *vals) {
+  if (m <= 0 || n <= 0 || !(density >= 0.0 && density < 1.0))
+    return 1;
+  ORC_DISPATCH(vtype, itype,
+               gen_random<T, I>(m, n, density, seed, (I *)rowptr, (I *)colind,
+                                (T *)vals));
+  return 0;
+}
+
+int64_t orc_band_csr_nnz(int64_t size, int64_t up, int64_t down) {
+  return (1 + up + down) * size - (up * (up + 1) / 2) - (down * (down + 1) / 2);
+}
+
+int orc_gen_band_csr(int vtype, int itype, int64_t size, int64_t up,
+                     int64_t down, void *rowptr, void *colind, void *vals) {
+  if (size <= 0 || up < 0 || down < 0)
+    return 1;
+  ORC_DISPATCH(vtype, itype,
+               gen_band<T, I>(size, up, down, (I *)rowptr, (I *)colind,
+                              (T *)vals));
+  return 0;
+}
+
+int orc_csr_gemv_row(int vtype, int itype, int acc, int64_t m, int64_t n,
+                     const void *rowptr, const void *colind, const void *vals,
+                     const void *x, int64_t k, void *y, int nseg) {
+  if (m < 0 || n < 0 || k < 1)
+    return 1;
+  ORC_DISPATCH(vtype, itype,
+               return dispatch_acc<T, I>(acc, 0, m, n, rowptr, colind, vals, x,
+                                         k, y, nseg));
+}
+
+int orc_csr_gemv_eq(int vtype, int itype, int acc, int64_t m, int64_t n,
+                    const void *rowptr, const void *colind, const void *vals,
+                    const void *x, int64_t k, void *y, int nseg) {
+  if (m <= 0 || n < 0 || k < 1)
+    return 1;
+  ORC_DISPATCH(vtype, itype,
+               return dispatch_acc<T, I>(acc, 1, m, n, rowptr, colind, vals, x,
+                                         k, y, nseg));
+}
+
+int orc_csr_gemv_row_threads(int vtype, int itype, int64_t m, int64_t n,
+                             const void *rowptr, const void *colind,
+                             const void *vals, const void *x, int64_t k,
+                             void *y, int nthreads, double *t_local,
+                             double *t_gather) {
+  if (m < 0 || k < 1 || nthreads < 1)
+    return 1;
+  ORC_DISPATCH(vtype, itype, {
+    int64_t P = nthreads;
+    int64_t seg = (m + P - 1) / P;
+    std::vector<std::vector<T>> partial(P);
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> th;
+    for (int64_t r = 0; r < P; r++) {
+      th.emplace_back([&, r] {
+        // Each "rank" allocates and zero-fills its partial result
+        // (csr_row_distribution.hpp:141-146) and runs the CPU loop.
+        partial[r].assign((size_t)std::max<int64_t>(seg * k, 1), (T)0);
+        gemv_row_segment<T, I, T, T>(m, n, (const I *)rowptr,
+                                     (const I *)colind, (const T *)vals,
+                                     (const T *)x, k, seg, r, partial[r].data());
+      });
+    }
+    for (auto &t : th)
+      t.join();
+    auto t1 = std::chrono::steady_clock::now();
+    T *Y = (T *)y;
+    for (int64_t r = 0; r < P; r++) {
+      if (r * seg >= m)
+        break;
+      int64_t cnt = std::min(seg, m - r * seg);
+      for (int64_t j = 0; j < k; j++)
+        std::memcpy(Y + m * j + r * seg, partial[r].data() + j * seg,
+                    sizeof(T) * cnt);
+    }
+    auto t2 = std::chrono::steady_clock::now();
+    if (t_local)
+      *t_local = std::chrono::duration<double>(t1 - t0).count();
+    if (t_gather)
+      *t_gather = std::chrono::duration<double>(t2 - t1).count();
+  });
+  return 0;
+}
+
+int orc_csr_absdot(int vtype, int itype, int64_t m, int64_t n,
+                   const void *rowptr, const void *colind, const void *vals,
+                   const void *x, int64_t k, double *d) {
+  ORC_DISPATCH(vtype, itype, {
+    auto R = (const I *)rowptr;
+    auto C = (const I *)colind;
+    auto V = (const T *)vals;
+    auto X = (const T *)x;
+    for (int64_t j = 0; j < k; j++)
+      for (int64_t r = 0; r < m; r++) {
+        long double s = 0;
+        for (int64_t p = (int64_t)R[r]; p < (int64_t)R[r + 1]; p++)
+          s += std::fabs((long double)V[p] * (long double)X[(int64_t)C[p] + j * n]);
+        d[r + j * m] = (double)s;
+      }
+  });
+  return 0;
+}
+
+int orc_dense_gemv(int vtype, int acc, int64_t m, int64_t n, const void *A,
+                   int64_t lda, const void *x, int64_t k, void *y) {
+  auto run = [&](auto tag, auto acc_tag) {
+    using T = decltype(tag);
+    using Acc = decltype(acc_tag);
+    auto a = (const T *)A;
+    auto X = (const T *)x;
+    for (int64_t j = 0; j < k; j++)
+      for (int64_t r = 0; r < m; r++) {
+        Acc s = 0;
+        for (int64_t c = 0; c < n; c++)
+          s += (Acc)a[r * lda + c] * (Acc)X[c + j * n];
+        if (acc == ORC_ACC_T)
+          ((T *)y)[r + j * m] = (T)s;
+        else
+          ((double *)y)[r + j * m] = (double)s;
+      }
+  };
+  if (vtype == ORC_F32) {
+    if (acc == ORC_ACC_T)
+      run(float(), float());
+    else if (acc == ORC_ACC_F64)
+      run(float(), double());
+    else
+      run(float(), (long double)0);
+  } else if (vtype == ORC_F64) {
+    if (acc == ORC_ACC_LD)
+      run(double(), (long double)0);
+    else
+      run(double(), double());
+  } else {
+    return 1;
+  }
+  return 0;
+}
+
+int orc_csr_transpose(int vtype, int itype, int64_t m, int64_t n,
+                      const void *rowptr, const void *colind, const void *vals,
+                      void *colptr, void *rowidx, void *vals_t) {
+  ORC_DISPATCH(vtype, itype, {
+    auto R = (const I *)rowptr;
+    auto C = (const I *)colind;
+    auto V = (const T *)vals;
+    auto CP = (I *)colptr;
+    auto RI = (I *)rowidx;
+    auto VT = (T *)vals_t;
+    int64_t nnz = (int64_t)R[m];
+    std::vector<int64_t> cnt(n + 1, 0);
+    for (int64_t p = 0; p < nnz; p++)
+      cnt[(int64_t)C[p] + 1]++;
+    for (int64_t c = 0; c < n; c++)
+      cnt[c + 1] += cnt[c];
+    for (int64_t c = 0; c <= n; c++)
+      CP[c] = (I)cnt[c];
+    for (int64_t r = 0; r < m; r++)
+      for (int64_t p = (int64_t)R[r]; p < (int64_t)R[r + 1]; p++) {
+        int64_t q = cnt[(int64_t)C[p]]++;
+        RI[q] = (I)r;
+        VT[q] = V[p];
+      }
+  });
+  return 0;
+}
+
+int orc_csr_abar(int vtype, int itype, int64_t m, const void *rowptr,
+                 const void *colind, const void *ybar, const void *x,
+                 double *abar) {
+  ORC_DISPATCH(vtype, itype, {
+    auto R = (const I *)rowptr;
+    auto C = (const I *)colind;
+    auto YB = (const T *)ybar;
+    auto X = (const T *)x;
+    for (int64_t r = 0; r < m; r++)
+      for (int64_t p = (int64_t)R[r]; p < (int64_t)R[r + 1]; p++)
+        abar[p] = (double)YB[r] * (double)X[(int64_t)C[p]];
+  });
+  return 0;
+}
+
+double orc_dot(int vtype, int64_t n, const void *a, const void *b) {
+  long double s = 0;
+  if (vtype == ORC_F32) {
+    auto A = (const float *)a;
+    auto B = (const float *)b;
+    for (int64_t i = 0; i < n; i++)
+      s += (long double)A[i] * (long double)B[i];
+  } else {
+    auto A = (const double *)a;
+    auto B = (const double *)b;
+    for (int64_t i = 0; i < n; i++)
+      s += (long double)A[i] * (long double)B[i];
+  }
+  return (double)s;
+}
+
+void orc_f32_to_bf16(int64_t n, const float *in, uint16_t *out) {
+  for (int64_t i = 0; i < n; i++) {
+    uint32_t u;
+    std::memcpy(&u, &in[i], 4);
+    if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x007fffffu)) {
+      out[i] = (uint16_t)((u >> 16) | 0x0040u); // quiet NaN
+    } else {
+      uint32_t lsb = (u >> 16) & 1u;
+      out[i] = (uint16_t)((u + 0x7fffu + lsb) >> 16);
+    }
+  }
+}
+
+void orc_bf16_to_f32(int64_t n, const uint16_t *in, float *out) {
+  for (int64_t i = 0; i < n; i++) {
+    uint32_t u = (uint32_t)in[i] << 16;
+    std::memcpy(&out[i], &u, 4);
+  }
+}
+
+} // extern "C"

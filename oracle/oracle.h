@@ -1,0 +1,129 @@
+/*
+ * oracle.h -- CPU restatement of Distributed Ranges' gemv hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load it.  Nothing in the product (distributed-ranges_b200/) links or calls
+ * it, and the product never falls back to it.
+ *
+ * Every function restates one piece of the reference's algorithm and cites
+ * the reference file:line it follows (paths are relative to the reference
+ * project root).  Value-type codes: 0 = float, 1 = double.  Index-type codes:
+ * 0 = int32, 1 = int64, 2 = uint64 (the reference tests' `unsigned long`).
+ *
+ * Accumulation modes for the gemv restatements:
+ *   ORC_ACC_T      accumulate in the value type T (the reference's own
+ *                  semantics: `T sum`, `res[...] += ...` in T);
+ *   ORC_ACC_F64    accumulate in double, output double;
+ *   ORC_ACC_LD     accumulate in x87 long double, output double (a near-exact
+ *                  FP64 oracle for error statistics).
+ */
+#ifndef DRB_ORACLE_H
+#define DRB_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_F32 = 0, ORC_F64 = 1 };
+enum { ORC_I32 = 0, ORC_I64 = 1, ORC_U64 = 2 };
+enum { ORC_ACC_T = 0, ORC_ACC_F64 = 1, ORC_ACC_LD = 2 };
+
+/* ---- generators (include/dr/detail/generate_csr.hpp) ------------------- */
+
+/* nnz that generate_random_csr produces: size_t(density * m * n)
+ * (generate_csr.hpp:48). */
+int64_t orc_random_csr_nnz(int64_t m, int64_t n, double density);
+
+/* Restates dr::generate_random_csr<T, I>(shape, density, seed)
+ * (generate_csr.hpp:40-103): mt19937(seed), row then column draws from
+ * uniform_int_distribution<I>, a uniform_real_distribution<T>(0,1) value for
+ * each new (row, col) pair, entries sorted by (row, col), then the CSR fill.
+ * Output buffers: rowptr[m+1], colind[nnz], vals[nnz] of the given types. */
+int orc_gen_random_csr(int vtype, int itype, int64_t m, int64_t n,
+                       double density, uint32_t seed, void *rowptr,
+                       void *colind, void *vals);
+
+/* nnz of generate_band_csr (generate_csr.hpp:111-113). */
+int64_t orc_band_csr_nnz(int64_t size, int64_t up, int64_t down);
+
+/* Restates dr::generate_band_csr<T, I>(size, up, down)
+ * (generate_csr.hpp:108-153): all values 1, columns i-down..i+up. */
+int orc_gen_band_csr(int vtype, int itype, int64_t size, int64_t up,
+                     int64_t down, void *rowptr, void *colind, void *vals);
+
+/* ---- gemv (csr_row / csr_eq CPU branches) ------------------------------ */
+
+/* y = A*x over `nseg` row-block segments, restating
+ * csr_row_distribution::local_gemv's CPU branch
+ * (include/dr/mp/containers/matrix_formats/csr_row_distribution.hpp:116-133)
+ * per segment plus gather_gemv_vector's reassembly (:159-204).
+ * x is n*k column-major (x[c + j*n]); y is m*k column-major (y[r + j*m]).
+ * With acc = ORC_ACC_T, y has the value type; otherwise y is double. */
+int orc_csr_gemv_row(int vtype, int itype, int acc, int64_t m, int64_t n,
+                     const void *rowptr, const void *colind, const void *vals,
+                     const void *x, int64_t k, void *y, int nseg);
+
+/* Same product over `nseg` equal-nnz segments, restating
+ * csr_eq_distribution::local_gemv's CPU branch
+ * (include/dr/mp/containers/matrix_formats/csr_eq_distribution.hpp:112-130),
+ * the row ranges of init (:253-272) and the gather that adds each segment's
+ * first (possibly split) row and copies the rest (:185-205). */
+int orc_csr_gemv_eq(int vtype, int itype, int acc, int64_t m, int64_t n,
+                    const void *rowptr, const void *colind, const void *vals,
+                    const void *x, int64_t k, void *y, int nseg);
+
+/* CPU baseline: the csr_row CPU loop run by `nthreads` std::threads, each
+ * owning the reference's row block ceil(m/P) (one thread stands in for one
+ * MPI rank).  Accumulates in T.  Returns elapsed seconds of the local phase in
+ * *t_local and of the gather (copy into y) in *t_gather. */
+int orc_csr_gemv_row_threads(int vtype, int itype, int64_t m, int64_t n,
+                             const void *rowptr, const void *colind,
+                             const void *vals, const void *x, int64_t k,
+                             void *y, int nthreads, double *t_local,
+                             double *t_gather);
+
+/* Per-row error denominators: d[r + j*m] = sum_p |a_p * x[col_p + j*n]|
+ * (double).  Used for relative-error gates under cancellation. */
+int orc_csr_absdot(int vtype, int itype, int64_t m, int64_t n,
+                   const void *rowptr, const void *colind, const void *vals,
+                   const void *x, int64_t k, double *d);
+
+/* ---- dense gemv (no reference symbol; row-dot restatement) ------------- */
+
+/* y[r + j*m] = sum_c A[r*lda + c] * x[c + j*n], accumulated per `acc`. */
+int orc_dense_gemv(int vtype, int acc, int64_t m, int64_t n, const void *A,
+                   int64_t lda, const void *x, int64_t k, void *y);
+
+/* ---- adjoint ----------------------------------------------------------- */
+
+/* Explicit CSR -> CSC transpose on the host (stable: rows ascending within
+ * a column).  Outputs colptr[n+1], rowidx[nnz], vals_t[nnz] in the input
+ * types. */
+int orc_csr_transpose(int vtype, int itype, int64_t m, int64_t n,
+                      const void *rowptr, const void *colind, const void *vals,
+                      void *colptr, void *rowidx, void *vals_t);
+
+/* abar[p] = ybar[row(p)] * x[col(p)] on the sparsity pattern (double). */
+int orc_csr_abar(int vtype, int itype, int64_t m, const void *rowptr,
+                 const void *colind, const void *ybar, const void *x,
+                 double *abar);
+
+/* ---- reductions (include/dr/mp/algorithms/reduce.hpp:9-20 std_reduce) -- */
+
+/* sum_i a[i]*b[i] accumulated in long double, returned as double. */
+double orc_dot(int vtype, int64_t n, const void *a, const void *b);
+
+/* ---- bf16 helpers -------------------------------------------------------- */
+
+/* Round-to-nearest-even float -> bfloat16 bits (NaN kept quiet). */
+void orc_f32_to_bf16(int64_t n, const float *in, uint16_t *out);
+void orc_bf16_to_f32(int64_t n, const uint16_t *in, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRB_ORACLE_H */

@@ -1,0 +1,409 @@
+"""GPU parity: the sm_100a kernels against the reference's own test cases
+(golden fixtures) and the CPU oracle, through the C ABI."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, name + ".npz")))
+
+
+@pytest.fixture(scope="module")
+def mp():
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from drb import mp as _mp
+    return _mp
+
+
+def view(mp, f):
+    return mp.csr_matrix_view(f["values"], f["rowptr"], f["colind"],
+                              (int(f["m"]), int(f["n"])))
+
+
+def rel_err(y, y_ref, denom):
+    d = np.maximum(np.asarray(denom, np.float64), np.finfo(np.float64).tiny)
+    return float(np.max(np.abs(np.asarray(y, np.float64) - y_ref) / d)) if len(d) else 0.0
+
+
+# ---- the reference tests' own cases (test/gtest/mp/gemv.cpp, sp/gemv.cpp) ----
+KAT = ["mp_gemv_100x100", "mp_gemv_1000x10", "mp_gemv_10x1000", "sp_very_sparse_100x100",
+       "sp_empty_100x100", "sp_zero_vector_100x100", "band_f32_100_3_3"]
+
+
+@pytest.mark.parametrize("name", KAT)
+@pytest.mark.parametrize("distr", ["row", "eq"])
+@pytest.mark.parametrize("nseg", [1, 3])
+def test_reference_gemv_cases(mp, name, distr, nseg):
+    f = load(name)
+    pol = mp.csr_row_distribution if distr == "row" else mp.csr_eq_distribution
+    a = mp.distributed_sparse_matrix(view(mp, f), 0, distr=pol, nsegments=nseg)
+    m, n = a.shape()
+    b = mp.broadcasted_vector()
+    b.broadcast_data(n, 0, f["x"], mp.default_comm())
+    c = [0.0] * m
+    mp.gemv(c, a, b)                      # no-root overload, gemv.hpp:41-55
+    assert oracle.fp_equal(f["expected"], np.array(c, np.float32))
+    c2 = np.zeros(m, np.float32)
+    mp.gemv(0, c2, a, b)                  # root overload, gemv.hpp:16-27
+    assert np.array_equal(np.array(c, np.float32), c2)
+
+
+@pytest.mark.parametrize("name", ["mp_gemv_100x100", "mp_gemv_1000x10", "mp_gemv_10x1000"])
+@pytest.mark.parametrize("distr", ["row", "eq"])
+def test_reference_gemm_width20(mp, name, distr):
+    f = load(name)
+    pol = mp.csr_row_distribution if distr == "row" else mp.csr_eq_distribution
+    a = mp.distributed_sparse_matrix(view(mp, f), 0, distr=pol, nsegments=2)
+    m, n = a.shape()
+    b = mp.broadcasted_slim_matrix()
+    b.broadcast_data(n, 20, 0, f["x_w20"], mp.default_comm())
+    c = np.zeros(m * 20, np.float32)
+    mp.gemv(0, c, a, b)                   # gemv.hpp:29-39
+    assert oracle.fp_equal(f["expected_w20"], c)
+
+
+@pytest.mark.parametrize("name", ["band_f64_1000_20_20", "band_f64_257_3_3"])
+def test_band_f64_exact(mp, name):
+    # examples/mp/sparse_matrix.cpp:84-102: res[i] != ref[i] is a mismatch
+    f = load(name)
+    for pol in (mp.csr_eq_distribution, mp.csr_row_distribution):
+        a = mp.distributed_sparse_matrix(view(mp, f), 0, distr=pol, nsegments=4)
+        b = mp.broadcasted_vector()
+        b.broadcast_data(a.shape()[1], 0, f["x"])
+        res = np.zeros(a.shape()[0], np.float64)
+        mp.gemv(0, res, a, b)
+        assert np.array_equal(res, f["expected"])
+
+
+def test_entries_iteration_matches_source(mp):
+    # IterRow/IterEq (test/gtest/mp/sparse_matrix.cpp): entry-wise equality
+    f = load("mp_gemv_100x100")
+    for pol in (mp.csr_row_distribution, mp.csr_eq_distribution):
+        a = mp.distributed_sparse_matrix(view(mp, f), 0, distr=pol, nsegments=3)
+        got = list(a)
+        src = list(mp.csr_matrix_view(f["values"], f["rowptr"], f["colind"], (100, 100)))
+        assert len(got) == len(src) == a.size()
+        for (i1, v1), (i2, v2) in zip(got, src):
+            assert i1 == i2 and np.float32(v1) == v2
+        total = sum(len(s) for s in a.segments())
+        assert total == a.size()
+        assert a[5] == got[5]
+
+
+def test_segments_follow_reference_rules(mp):
+    f = load("mp_gemv_1000x10")
+    rp = f["rowptr"].astype(np.int64)
+    m, nnz = 1000, int(rp[-1])
+    for P in (1, 2, 3, 7):
+        a = mp.distributed_sparse_matrix(view(mp, f), 0, distr=mp.csr_row_distribution,
+                                         nsegments=P)
+        seg = -(-m // P)
+        for r, s in enumerate(a.segments()):
+            r0, r1 = min(m, r * seg), min(m, (r + 1) * seg)
+            assert (s.row_begin, s.row_end) == (r0, r1)
+            assert (s.nnz_begin, s.nnz_end) == (rp[r0], rp[r1])
+        a = mp.distributed_sparse_matrix(view(mp, f), 0, distr=mp.csr_eq_distribution,
+                                         nsegments=P)
+        seg = -(-nnz // P)
+        for r, s in enumerate(a.segments()):
+            z0, z1 = min(nnz, r * seg), min(nnz, (r + 1) * seg)
+            assert (s.nnz_begin, s.nnz_end) == (z0, z1)
+            if z0 < z1:
+                assert s.row_begin == np.searchsorted(rp[:m], z0, side="right") - 1
+                assert s.row_end == np.searchsorted(rp[:m], z1 - 1, side="right")
+
+
+# ---- parity against the FP64 oracle at the benchmark shapes ---------------------
+def gpu_gemv(mp, rp, ci, v, m, n, x, k=1, layout=0, **kw):
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0, **kw)
+    xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    yt = torch.empty(m * k, dtype=xt.dtype, device="cuda")
+    a.gemv_device(xt, yt, k, layout)
+    torch.cuda.synchronize()
+    return a, yt.cpu().numpy()
+
+
+def test_fixed16_fp32_vs_fp64_oracle(mp):
+    # 131072 x 131072, exactly 16 distinct sorted uniform columns per row
+    import drb
+    m = 131072
+    rp, ci, v = drb.gen.fixed_rows_csr(m, m, length=16, seed=20261204)
+    x = drb.gen.values(m, seed=77)
+    _, y = gpu_gemv(mp, rp, ci, v, m, m, x)
+    y64 = oracle.gemv_row(rp, ci, v, x, m, m, 1, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v, x, m, m)
+    assert rel_err(y, y64, d) <= 1e-5
+    y32 = oracle.gemv_row(rp, ci, v, x, m, m)   # the reference's own fp32 loop
+    assert rel_err(y, y32.astype(np.float64), d) <= 1e-5
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_powerlaw_long_rows(mp, dtype):
+    import drb
+    m = 300_000
+    a_ = drb.gen.zipf_alpha_for_mean(1, 16384, 20.0)
+    rp, ci, v = drb.gen.powerlaw_csr(m, m, alpha=a_, hi=16384, seed=5, value_dtype=dtype)
+    assert np.diff(rp).max() > 2048     # long rows are exercised
+    x = drb.gen.values(m, seed=6, dtype=dtype)
+    _, y = gpu_gemv(mp, rp, ci, v, m, m, x)
+    y64 = oracle.gemv_row(rp, ci, v, x, m, m, 1, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v, x, m, m)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert rel_err(y, y64, d) <= tol
+
+
+def chunky_matrix(dtype, idx=np.int32):
+    """Rows of every kind: empty, short, tile-boundary, long, and two rows
+    longer than one CTA's chunk limit (chunked with a ticketed finish)."""
+    rng = np.random.default_rng(3)
+    n = 400_000
+    lens = np.concatenate([
+        rng.integers(0, 40, 5000), [2047, 2048, 2049, 0, 0, 1], [70_000, 0, 300_001],
+        rng.integers(0, 5, 3000), [65536, 65537], rng.integers(100, 3000, 200)])
+    m = len(lens)
+    rp = np.zeros(m + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.empty(rp[-1], idx)
+    for r in range(m):
+        L = lens[r]
+        if L:
+            ci[rp[r]:rp[r + 1]] = np.sort(rng.choice(n, L, replace=False))
+    v = rng.uniform(-1, 1, rp[-1]).astype(dtype)
+    return rp.astype(idx), ci, v, m, n
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_chunked_rows_deterministic(mp, dtype):
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    x = np.random.default_rng(4).uniform(-1, 1, n).astype(dtype)
+    a, y1 = gpu_gemv(mp, rp, ci, v, m, n, x)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.empty(m, dtype=xt.dtype, device="cuda")
+    for _ in range(3):  # counters must be re-armed between launches
+        a.gemv_device(xt, yt)
+    torch.cuda.synchronize()
+    assert np.array_equal(y1.view(np.uint8), yt.cpu().numpy().view(np.uint8))
+    y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v, x, m, n)
+    assert rel_err(y1, y64, d) <= (1e-5 if dtype == np.float32 else 1e-12)
+
+
+@pytest.mark.parametrize("keep64", [False, True])
+def test_int64_indices(mp, keep64):
+    rp, ci, v, m, n = chunky_matrix(np.float64, np.int64)
+    x = np.random.default_rng(8).standard_normal(n)
+    a, y = gpu_gemv(mp, rp, ci, v, m, n, x, keep_index64=keep64)
+    vb, cb, rb = a.storage_bytes()
+    assert (vb, cb) == (8, 8 if keep64 else 4)
+    y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
+    assert rel_err(y, y64, oracle.absdot(rp, ci, v, x, m, n)) <= 1e-12
+
+
+@pytest.mark.parametrize("k", [2, 3, 8, 16, 33])
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_multi_rhs(mp, k, layout, dtype):
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    rng = np.random.default_rng(k)
+    X = rng.uniform(-1, 1, (n, k)).astype(dtype)           # X[c, j]
+    xin = X.T.ravel() if layout == 0 else X.ravel()
+    _, y = gpu_gemv(mp, rp, ci, v, m, n, xin, k, layout)
+    Y = y.reshape(k, m).T if layout == 0 else y.reshape(m, k)
+    y64 = oracle.gemv_row(rp, ci, v, X.T.ravel(), m, n, k, oracle.ACC_LD).reshape(k, m).T
+    d = oracle.absdot(rp, ci, v, X.T.ravel(), m, n, k).reshape(k, m).T
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert rel_err(Y.ravel(), y64.ravel(), d.ravel()) <= tol
+
+
+def test_host_gemv_matches_device(mp):
+    import drb
+    m = 50_000
+    rp, ci, v = drb.gen.uniform_rows_csr(m, m, lo=8, hi=64, seed=2)
+    x = drb.gen.values(m, seed=3)
+    a, y_dev = gpu_gemv(mp, rp, ci, v, m, m, x)
+    xh = torch.from_numpy(x).pin_memory()
+    yh = torch.empty(m, dtype=torch.float32).pin_memory()
+    a.gemv_host(xh.numpy(), yh.numpy())
+    assert np.array_equal(yh.numpy(), y_dev)
+
+
+@pytest.mark.parametrize("m,n", [(1, 1), (2, 3), (31, 33), (32, 32), (33, 31), (1, 5000)])
+def test_ragged_small_shapes(mp, m, n):
+    rp, ci, v = oracle.random_csr(m, n, 0.5 if m * n > 1 else 0.0, 1, np.float64, np.int64)
+    if m * n == 1:
+        rp, ci, v = np.array([0, 1], np.int64), np.array([0], np.int64), np.array([2.5])
+    x = np.random.default_rng(0).standard_normal(n)
+    _, y = gpu_gemv(mp, rp, ci, v, m, n, x)
+    y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
+    assert rel_err(y, y64, oracle.absdot(rp, ci, v, x, m, n)) <= 1e-12
+
+
+def test_bad_csr_rejected(mp):
+    from drb._capi import DrbError, DRB_ERR_BAD_CSR
+    rp = np.array([0, 2, 1, 3], np.int32)
+    ci = np.array([0, 1, 2], np.int32)
+    v = np.ones(3, np.float32)
+    with pytest.raises(DrbError) as e:
+        mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (3, 3)), 0)
+    assert e.value.status == DRB_ERR_BAD_CSR
+    rp = np.array([0, 1, 2, 3], np.int32)
+    ci = np.array([0, 3, 1], np.int32)      # column 3 of a 3-column matrix
+    with pytest.raises(DrbError) as e:
+        mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (3, 3)), 0)
+    assert e.value.status == DRB_ERR_BAD_CSR
+
+
+def test_gemv_size_mismatch_raises(mp):
+    f = load("mp_gemv_100x100")
+    a = mp.distributed_sparse_matrix(view(mp, f), 0)
+    b = mp.broadcasted_vector()
+    b.broadcast_data(100, 0, f["x"])
+    with pytest.raises(ValueError):
+        mp.gemv(0, [0.0] * 99, a, b)
+    with pytest.raises(ValueError):
+        mp.gemv(1, [0.0] * 100, a, b)
+
+
+# ---- dense gemv, dot, fused residual ------------------------------------------
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("m,n,k,pad", [(257, 1024, 1, 0), (300, 777, 1, 3), (129, 512, 3, 0),
+                                       (64, 96, 8, 4), (65, 100, 9, 0), (5, 1, 1, 0)])
+@pytest.mark.parametrize("layout", [0, 1])
+def test_dense_gemv(mp, dtype, m, n, k, pad, layout):
+    g = torch.Generator().manual_seed(m * 7 + n)
+    A_full = torch.randn(m, n + pad, generator=g, dtype=torch.float64)
+    X = torch.randn(n, k, generator=g, dtype=torch.float64)
+    A = A_full.to(dtype).cuda()[:, :n]
+    xin = (X.t().contiguous() if layout == 0 else X.contiguous()).to(dtype).cuda()
+    y = torch.empty(m * k, dtype=dtype, device="cuda")
+    mp.dense_gemv(A, xin, y, k, layout)
+    torch.cuda.synchronize()
+    Y = y.cpu().view(k, m).t() if layout == 0 else y.cpu().view(m, k)
+    ref = oracle.dense_gemv(A.cpu().double().contiguous().numpy(),
+                            X.to(dtype).double().t().contiguous().numpy().ravel(), k,
+                            oracle.ACC_LD).reshape(k, m).T
+    denom = (A.cpu().double().abs() @ X.to(dtype).double().abs()).numpy()
+    tol = 1e-5 if dtype == torch.float32 else 1e-12
+    assert rel_err(Y.double().numpy().ravel(), ref.ravel(), denom.ravel()) <= tol
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("n", [0, 1, 7, 1000, 1 << 20, (1 << 20) + 3])
+def test_dot(mp, dtype, n):
+    g = torch.Generator().manual_seed(n)
+    a = torch.randn(n, generator=g, dtype=torch.float64).to(dtype)
+    b = torch.randn(n, generator=g, dtype=torch.float64).to(dtype)
+    out = mp.dot(a.cuda(), b.cuda())
+    out2 = mp.dot(a.cuda(), b.cuda())
+    ref = oracle.dot(a.numpy(), b.numpy())
+    got = float(out.item())
+    assert got == float(out2.item())        # deterministic
+    assert abs(got - ref) <= 1e-12 * max(1.0, float((a.double().abs() * b.double().abs()).sum()))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_residual_norm2(mp, dtype):
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    rng = np.random.default_rng(1)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    b = rng.uniform(-1, 1, m).astype(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    y = torch.empty(m, dtype=torch.from_numpy(x).dtype, device="cuda")
+    out = mp.residual_norm2(a, torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda(), y)
+    out2 = mp.residual_norm2(a, torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda())
+    y_gpu = y.cpu().numpy().astype(np.float64)
+    ref = float(((y_gpu - b.astype(np.float64)) ** 2).sum())
+    assert abs(out.item() - ref) <= 1e-10 * ref
+    assert out.item() == out2.item()
+    y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
+    assert rel_err(y_gpu, y64, oracle.absdot(rp, ci, v, x, m, n)) <= (
+        1e-5 if dtype == np.float32 else 1e-12)
+
+
+# ---- adjoint ------------------------------------------------------------------------
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_adjoint_against_transposed_oracle(mp, dtype):
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    rng = np.random.default_rng(2)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    yb = rng.uniform(-1, 1, m).astype(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0, adjoint=True)
+    tdt = torch.from_numpy(x).dtype
+    xbar = torch.empty(n, dtype=tdt, device="cuda")
+    abar = torch.empty(len(v), dtype=tdt, device="cuda")
+    mp.gemv_backward(a, torch.from_numpy(yb).cuda(), torch.from_numpy(x).cuda(), xbar, abar)
+    torch.cuda.synchronize()
+    cp, ri, vt = oracle.transpose(rp, ci, v, m, n)
+    xb_ref = oracle.gemv_row(cp, ri, vt, yb, n, m, 1, oracle.ACC_LD)
+    d = oracle.absdot(cp, ri, vt, yb, n, m)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert rel_err(xbar.cpu().numpy(), xb_ref, d) <= tol
+    ab_ref = oracle.abar(rp, ci, yb, x, m)
+    assert np.allclose(abar.cpu().numpy(), ab_ref, rtol=1e-6 if dtype == np.float32 else 1e-15,
+                       atol=0)
+    # values updated in CSR order must reach the transposed copy
+    v2 = (v * 2).astype(dtype)
+    a.update_values(torch.from_numpy(v2).cuda())
+    mp.gemv_backward(a, torch.from_numpy(yb).cuda(), None, xbar, None)
+    torch.cuda.synchronize()
+    assert rel_err(xbar.cpu().numpy(), 2 * xb_ref, 2 * d) <= tol
+
+
+def test_adjoint_finite_differences_laplacian(mp):
+    import drb
+    g = 48
+    rp, ci, v = drb.gen.laplacian2d_csr(g, value_dtype=np.float64)
+    m = g * g
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal(m)
+    b = rng.standard_normal(m)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, m)), 0, adjoint=True)
+    xt, bt = torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda()
+    y = torch.empty(m, dtype=torch.float64, device="cuda")
+    a.gemv_device(xt, y)
+    r = y - bt
+    xbar = torch.empty(m, dtype=torch.float64, device="cuda")
+    abar = torch.empty(len(v), dtype=torch.float64, device="cuda")
+    mp.gemv_backward(a, r, xt, xbar, abar)
+    L = lambda xx: 0.5 * mp.residual_norm2(a, xx, bt).item()
+    h = 1e-6
+    for i in rng.choice(m, 32, replace=False):
+        e = torch.zeros(m, dtype=torch.float64, device="cuda")
+        e[i] = h
+        fd = (L(xt + e) - L(xt - e)) / (2 * h)
+        assert abs(fd - xbar[i].item()) <= 1e-6 * max(1.0, abs(fd))
+    # dL/dA_p by perturbing one stored value
+    vt = torch.from_numpy(v.copy()).cuda()
+    for p in rng.choice(len(v), 8, replace=False):
+        vp, vm = vt.clone(), vt.clone()
+        vp[p] += h
+        vm[p] -= h
+        a.update_values(vp)
+        lp = L(xt)
+        a.update_values(vm)
+        lm = L(xt)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - abar[p].item()) <= 1e-6 * max(1.0, abs(fd))
+    a.update_values(vt)
+
+
+def test_launch_count_increases(mp):
+    from drb import _capi
+    f = load("mp_gemv_100x100")
+    a = mp.distributed_sparse_matrix(view(mp, f), 0)
+    b = mp.broadcasted_vector()
+    b.broadcast_data(100, 0, f["x"])
+    c0 = _capi.launch_count()
+    mp.gemv(0, np.zeros(100, np.float32), a, b)
+    assert _capi.launch_count() == c0 + 1
