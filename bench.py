@@ -213,7 +213,8 @@ def run_ours(args):
     nnz = int(rp[-1])
     stream = torch.cuda.current_stream()
     A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (M, N_COLS)), 0,
-                                     distr=mp.csr_row_distribution, adjoint=True)
+                                     distr=mp.csr_row_distribution,
+                                     adjoint=not args.no_extra, autotune=True)
     vb, cb, rb = A.storage_bytes()
     bytes_ = alg_bytes(M, N_COLS, nnz, vb, cb, rb, 4, 4)
     xd = torch.from_numpy(x).cuda()

@@ -166,7 +166,8 @@ drb_status build_typed(Csr &A, cudaStream_t s) {
   T.cbytes = A.cbytes;
   T.rbytes = A.rbytes;
   const int64_t nnz = A.nnz, pad = ((nnz + kPadElems - 1) / kPadElems + 1) * kPadElems;
-  DRB_TRY(T.rowptr.alloc(sizeof(RI) * (A.n + 1)));
+  DRB_TRY(T.rowptr.alloc(sizeof(RI) * (A.n + 1 + kRowptrPad)));
+  DRB_CUDA_TRY(cudaMemsetAsync(T.rowptr.p, 0, T.rowptr.bytes, s));
   DRB_TRY(T.colind.alloc(sizeof(CI) * pad));
   DRB_TRY(T.vals.alloc(sizeof(V) * pad));
   DRB_CUDA_TRY(cudaMemsetAsync(T.colind.p, 0, T.colind.bytes, s));
@@ -208,6 +209,8 @@ drb_status build_typed(Csr &A, cudaStream_t s) {
   keys_out.release();
   DRB_TRY(build_plan(T.plan, T.m, cp.data(), sizeof(RI),
                      plan_group(dtype_bytes(T.storage), T.cbytes), 0, 0, 0));
+  DRB_TRY(build_pipe_plan(T.pipe, T.m, cp.data(), sizeof(RI),
+                          plan_group(dtype_bytes(T.storage), T.cbytes), 0, 0));
   return DRB_OK;
 }
 

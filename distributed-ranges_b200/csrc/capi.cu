@@ -42,7 +42,15 @@ drb_status invalid(const char *msg) {
   return DRB_ERR_INVALID_ARG;
 }
 
+// Device checks are cached per device: cudaGetDeviceProperties costs tens of
+// microseconds, too much for every call of a sub-millisecond kernel.
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_dev_ok[kMaxDevices];
+
 drb_status check_device(int *dev) {
+  if (cudaGetDevice(dev) == cudaSuccess && *dev >= 0 && *dev < kMaxDevices &&
+      g_dev_ok[*dev].load(std::memory_order_relaxed) == 1)
+    return DRB_OK;
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
@@ -58,6 +66,8 @@ drb_status check_device(int *dev) {
               *dev, prop.major, prop.minor);
     return DRB_ERR_NO_DEVICE;
   }
+  if (*dev >= 0 && *dev < kMaxDevices)
+    g_dev_ok[*dev].store(1, std::memory_order_relaxed);
   return DRB_OK;
 }
 
@@ -322,7 +332,8 @@ drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
   A->rbytes = (ib == 8 && ((flags & DRB_FLAG_KEEP_INDEX64) || nnz > 0x7fffffff)) ? 8 : 4;
   const int vb_in = dtype_bytes(value_type), vb = dtype_bytes(storage);
   const int64_t pad = ((nnz + kPadElems - 1) / kPadElems + 1) * kPadElems;
-  DRB_TRY(A->rowptr.alloc((size_t)A->rbytes * (m + 1)));
+  DRB_TRY(A->rowptr.alloc((size_t)A->rbytes * (m + 1 + kRowptrPad)));
+  DRB_CUDA_TRY(cudaMemsetAsync(A->rowptr.p, 0, A->rowptr.bytes, s));
   DRB_TRY(A->colind.alloc((size_t)A->cbytes * pad));
   DRB_TRY(A->vals.alloc((size_t)vb * pad));
   DRB_CUDA_TRY(cudaMemsetAsync(A->colind.p, 0, A->colind.bytes, s));
@@ -333,10 +344,16 @@ drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
                  storage == DRB_BF16, s));
   DRB_CUDA_TRY(cudaStreamSynchronize(s));
   DRB_TRY(build_plan(A->plan, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0, 0));
+  DRB_TRY(build_pipe_plan(A->pipe, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0));
   compute_segments(*A, rp_h, ib);
   if (flags & DRB_FLAG_ADJOINT) {
     DRB_TRY(adjoint_build(*A, s));
     DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if ((flags & DRB_FLAG_AUTOTUNE) && storage != DRB_BF16 && nnz > 0) {
+    DRB_TRY(autotune_pipe(*A, s, nullptr));
+    if (A->tr)
+      DRB_TRY(autotune_pipe(*A->tr, s, nullptr));
   }
   *out = A.release();
   return DRB_OK;
@@ -536,6 +553,40 @@ drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
   return DRB_OK;
 }
 
+drb_status drb_csr_variant(drb_csr_t A, int *variant) {
+  if (!A || !variant)
+    return invalid("NULL argument");
+  *variant = A->pipe.tile | (A->pipe.skew ? 1 : 0);
+  return DRB_OK;
+}
+
+drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  DeviceGuard g(A->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int v = 0;
+  DRB_TRY(autotune_pipe(*A, s, &v));
+  if (A->tr)
+    DRB_TRY(autotune_pipe(*A->tr, s, nullptr));
+  if (variant)
+    *variant = v;
+  return DRB_OK;
+}
+
+drb_status drb_csr_check(drb_csr_t A, void *stream) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  DeviceGuard g(A->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DRB_TRY(pipe_check(*A, s));
+  if (A->tr)
+    DRB_TRY(pipe_check(*A->tr, s));
+  return DRB_OK;
+}
+
 drb_status drb_csr_update_values(drb_csr_t A, const void *values,
                                  void *stream) {
   clear_error();
@@ -565,6 +616,65 @@ drb_status drb_dense_gemv(int64_t m, int64_t n, const void *Am, int64_t lda,
   DRB_TRY(check_device(&dev));
   return dense_launch(m, n, Am, lda, x, y, k, layout, dtype,
                       static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_malloc(void **ptr, size_t bytes) {
+  clear_error();
+  if (!ptr)
+    return invalid("ptr is NULL");
+  *ptr = nullptr;
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  DRB_CUDA_TRY(cudaMalloc(ptr, bytes ? bytes : 16));
+  return DRB_OK;
+}
+
+drb_status drb_free(void *ptr) {
+  clear_error();
+  if (ptr)
+    DRB_CUDA_TRY(cudaFree(ptr));
+  return DRB_OK;
+}
+
+drb_status drb_memcpy(void *dst, const void *src, size_t bytes, int kind,
+                      void *stream) {
+  clear_error();
+  if (bytes == 0)
+    return DRB_OK;
+  if (!dst || !src)
+    return invalid("NULL pointer");
+  cudaMemcpyKind k;
+  switch (kind) {
+  case 0:
+    k = cudaMemcpyHostToDevice;
+    break;
+  case 1:
+    k = cudaMemcpyDeviceToHost;
+    break;
+  case 2:
+    k = cudaMemcpyDeviceToDevice;
+    break;
+  default:
+    return invalid("memcpy kind");
+  }
+  DRB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, k, static_cast<cudaStream_t>(stream)));
+  return DRB_OK;
+}
+
+drb_status drb_memset(void *dst, int value, size_t bytes, void *stream) {
+  clear_error();
+  if (bytes == 0)
+    return DRB_OK;
+  if (!dst)
+    return invalid("NULL pointer");
+  DRB_CUDA_TRY(cudaMemsetAsync(dst, value, bytes, static_cast<cudaStream_t>(stream)));
+  return DRB_OK;
+}
+
+drb_status drb_stream_synchronize(void *stream) {
+  clear_error();
+  DRB_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  return DRB_OK;
 }
 
 drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,

@@ -213,13 +213,24 @@ __global__ void __launch_bounds__(kDotNT)
     s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
+  if (s_last) {
+    // the last CTA adds the partials with all threads in a fixed order
     __threadfence();
     double s = 0.0;
-    for (int i = 0; i < (int)gridDim.x; i++)
-      s += *(volatile double *)&partials[i];
-    *out = s;
-    *ticket = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += kDotNT)
+      s += __ldcg(&partials[i]);
+    s = warp_sum_d(s);
+    __syncthreads();
+    if (lane == 0)
+      s_red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kDotNT / 32; w++)
+        t += s_red[w];
+      *out = t;
+      *ticket = 0;
+    }
   }
 }
 

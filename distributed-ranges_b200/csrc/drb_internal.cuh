@@ -92,6 +92,41 @@ struct Plan {
   DevBuf red;          // double[nblocks] + int ticket: residual reduction
 };
 
+// Work item of the persistent SpMV (32 bytes).  Every item covers at most
+// `tile` elements of colind/values counted from the 16-byte aligned start
+// (p0 rounded down to the vector group):
+//   nrows > 0 : whole rows [r0, r0 + nrows), nnz [p0, p0 + len);
+//   nrows == 0: one chunk of row r0, nnz [p0, p0 + len); chunk indexes the
+//               Chunk table (partials + ticket finish, as in Plan).
+struct Item {
+  int64_t p0;
+  int32_t len;
+  int32_t r0;
+  int32_t nrows;
+  int32_t chunk;
+  int32_t pad0, pad1;
+};
+static_assert(sizeof(Item) == 32, "Item is 32 bytes");
+
+struct PipePlan {
+  int tile = 0, rows = 0, group = 0;
+  bool skew = false; // skewed product layout in the row reduction
+  int64_t nitems = 0, nchunks = 0, nsplit = 0;
+  DevBuf items;    // Item[nitems]
+  DevBuf chunks;   // Chunk[nchunks]
+  DevBuf partials; // value type [nchunks]
+  DevBuf counters; // int[nsplit]
+  DevBuf err;      // int: device-side error word (DRB_ERR_TIMEOUT)
+  DevBuf red;      // double[grid] + int ticket: fused residual
+};
+
+drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
+                           int rbytes, int group, int tile, int rows);
+
+// rowptr buffers carry this many extra zeroed elements past rowptr[m] so a
+// 16-byte-rounded bulk copy of a rowptr slice stays inside the allocation.
+constexpr int64_t kRowptrPad = 8;
+
 struct Csr {
   int device = 0;
   int64_t m = 0, n = 0, nnz = 0;
@@ -102,7 +137,8 @@ struct Csr {
   drb_partition part = DRB_PART_ROW;
   uint32_t flags = 0;
   DevBuf rowptr, colind, vals;
-  Plan plan;
+  Plan plan;      // row blocks: multi-RHS kernel and abar
+  PipePlan pipe;  // work items: the persistent single-RHS kernel
   std::vector<int64_t> seg_row0, seg_row1, seg_nz0, seg_nz1;
   // adjoint plan: A^T as a CSR matrix of shape n x m (colptr, rowidx, values
   // in column order, its own row-block plan) and perm[nnz] (CSC position ->
@@ -126,6 +162,11 @@ drb_status build_plan(Plan &plan, int64_t m, const void *rowptr_host,
 drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
                        drb_layout layout, cudaStream_t s);
 drb_status spmv_t_launch(Csr &A, const void *ybar, void *xbar, cudaStream_t s);
+drb_status spmv_pipe_launch(Csr &A, const void *x, void *y, cudaStream_t s);
+drb_status residual_pipe_launch(Csr &A, const void *x, const void *b, void *y,
+                                double *out, cudaStream_t s);
+drb_status pipe_check(Csr &A, cudaStream_t s);
+drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen);
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
                        cudaStream_t s);
 drb_status residual_launch(Csr &A, const void *x, const void *b, void *y,

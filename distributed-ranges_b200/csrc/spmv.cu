@@ -540,6 +540,8 @@ drb_status build_plan(Plan &plan, int64_t m, const void *rowptr_host,
 
 drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
                        drb_layout layout, cudaStream_t s) {
+  if (k == 1 && (A.storage == DRB_F32 || A.storage == DRB_F64))
+    return spmv_pipe_launch(A, x, y, s);
   switch (A.storage) {
   case DRB_F32:
     return dispatch_idx<float>(A, x, y, k, layout, nullptr, s);
@@ -553,6 +555,14 @@ drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
 
 drb_status residual_launch(Csr &A, const void *x, const void *b, void *y,
                            double *out, cudaStream_t s) {
+  if (A.storage == DRB_F32 || A.storage == DRB_F64) {
+    void *yt = y;
+    if (!yt) {
+      DRB_TRY(A.ys.ensure((size_t)dtype_bytes(A.storage) * A.m));
+      yt = A.ys.p;
+    }
+    return residual_pipe_launch(A, x, b, yt, out, s);
+  }
   Plan &P = A.plan;
   if (P.nblocks == 0) {
     DRB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double), s));

@@ -40,6 +40,7 @@ DRB_FLAG_KEEP_INDEX64 = 0x2
 DRB_FLAG_SKIP_VALIDATE = 0x4
 DRB_FLAG_ADJOINT = 0x8
 DRB_FLAG_COMPENSATED = 0x10
+DRB_FLAG_AUTOTUNE = 0x20
 
 STATUS_NAMES = {
     0: "DRB_OK", 1: "DRB_ERR_INVALID_ARG", 2: "DRB_ERR_BAD_CSR",
@@ -75,11 +76,19 @@ DRB_SYMBOLS = [
     ("drb_csr_get_entries", _st, [_vp, _i64, _i64, _vp, _vp, _vp]),
     ("drb_csr_gemv", _st, [_vp, _vp, _vp, _i64, _i32, _vp]),
     ("drb_csr_gemv_host", _st, [_vp, _vp, _vp, _i64, _i32, _vp]),
+    ("drb_csr_check", _st, [_vp, _vp]),
+    ("drb_csr_variant", _st, [_vp, C.POINTER(_i32)]),
+    ("drb_csr_autotune", _st, [_vp, C.POINTER(_i32), _vp]),
     ("drb_csr_residual_norm2", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("drb_csr_gemv_backward", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("drb_csr_update_values", _st, [_vp, _vp, _vp]),
     ("drb_dense_gemv", _st, [_i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _i32, _vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
+    ("drb_malloc", _st, [C.POINTER(_vp), C.c_size_t]),
+    ("drb_free", _st, [_vp]),
+    ("drb_memcpy", _st, [_vp, _vp, C.c_size_t, _i32, _vp]),
+    ("drb_memset", _st, [_vp, _i32, C.c_size_t, _vp]),
+    ("drb_stream_synchronize", _st, [_vp]),
     ("drb_last_error", C.c_char_p, []),
     ("drb_version", C.c_char_p, []),
     ("drb_launch_count", C.c_uint64, []),

@@ -189,7 +189,8 @@ class distributed_sparse_matrix:
     def __init__(self, csr_view, root: int = 0, dist: distribution | None = None,
                  *, distr=csr_eq_distribution, nsegments: int = 1,
                  storage=None, adjoint: bool = False,
-                 keep_index64: bool = False, stream=None):
+                 keep_index64: bool = False, autotune: bool = False,
+                 stream=None):
         if root != 0:
             raise ValueError(f"root {root} is not a rank: one process owns the GPU")
         self._h = C.c_void_p(0)
@@ -215,6 +216,8 @@ class distributed_sparse_matrix:
             flags |= capi.DRB_FLAG_ADJOINT
         if keep_index64:
             flags |= capi.DRB_FLAG_KEEP_INDEX64
+        if autotune:
+            flags |= capi.DRB_FLAG_AUTOTUNE
         h = C.c_void_p()
         check(capi.lib.drb_csr_create(
             C.byref(h), m, n, nnz, _ptr(rowptr), _ptr(colind), _ptr(values),
@@ -307,6 +310,22 @@ class distributed_sparse_matrix:
                   layout: int = capi.DRB_COL_MAJOR, stream=None) -> None:
         check(capi.lib.drb_csr_gemv_host(self._h, _ptr(x_host), _ptr(y_host),
                                          int(k), layout, _stream(stream)))
+
+    def variant(self) -> int:
+        """Single-RHS kernel variant: item span (256/512) | 1 if skewed."""
+        v = C.c_int()
+        check(capi.lib.drb_csr_variant(self._h, C.byref(v)))
+        return v.value
+
+    def autotune(self, stream=None) -> int:
+        """Time the kernel variants on this sparsity pattern, keep the best."""
+        v = C.c_int()
+        check(capi.lib.drb_csr_autotune(self._h, C.byref(v), _stream(stream)))
+        return v.value
+
+    def check(self, stream=None) -> None:
+        """Synchronise and raise DrbError if an earlier launch timed out."""
+        check(capi.lib.drb_csr_check(self._h, _stream(stream)))
 
     def update_values(self, values: torch.Tensor, stream=None) -> None:
         check(capi.lib.drb_csr_update_values(self._h, _ptr(values), _stream(stream)))
@@ -413,6 +432,8 @@ def gemv(*args, stream=None) -> None:
         root = 0
     else:
         raise TypeError("gemv(root, res, A, b) or gemv(res, A, b)")
+    if root != default_comm().rank():
+        raise ValueError(f"root {root} is not a rank: one process owns the GPU")
     m, n = a.shape()
     if isinstance(b, broadcasted_slim_matrix):
         width = b.width()

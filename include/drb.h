@@ -74,6 +74,7 @@ typedef enum { DRB_PART_ROW = 0, DRB_PART_EQ = 1 } drb_partition;
 #define DRB_FLAG_SKIP_VALIDATE 0x4u  /* skip the host-side CSR validation    */
 #define DRB_FLAG_ADJOINT 0x8u        /* build the CSC plan for gemv_backward */
 #define DRB_FLAG_COMPENSATED 0x10u   /* two-sum compensated FP32 row sums    */
+#define DRB_FLAG_AUTOTUNE 0x20u      /* run drb_csr_autotune at create       */
 
 typedef struct drb_csr_matrix *drb_csr_t;
 
@@ -133,6 +134,20 @@ drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
 drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
                              int64_t k, drb_layout layout, void *stream);
 
+/* Kernel variant of the single right-hand-side product: item span (256 or
+ * 512 nonzeros) | 1 when the skewed (bank-conflict-free) product layout is
+ * used.  drb_csr_autotune times the four variants on this matrix's sparsity
+ * pattern, keeps the fastest (also for the adjoint's transposed matrix) and
+ * returns it; it synchronises `stream`.  Results are identical across
+ * variants up to the summation order inside a row. */
+drb_status drb_csr_variant(drb_csr_t A, int *variant);
+drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
+
+/* Synchronise `stream` and report device-side failures of earlier launches
+ * on this handle: DRB_ERR_TIMEOUT when a bounded in-kernel wait expired (the
+ * kernel then skipped the rest of its work; the error word is cleared). */
+drb_status drb_csr_check(drb_csr_t A, void *stream);
+
 /* Fused residual: out[0] = || A*x - b ||_2^2 accumulated in f64 (device
  * double*), y = A*x also written when y != NULL.  k = 1. */
 drb_status drb_csr_residual_norm2(drb_csr_t A, const void *x, const void *b,
@@ -164,6 +179,20 @@ drb_status drb_dense_gemv(int64_t m, int64_t n, const void *A, int64_t lda,
  * with a deterministic order; out is a device double*.  F32 or F64. */
 drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
                    double *out, void *stream);
+
+/* ---- device memory (the reference's allocator and sycl_copy) --------------
+ * Replaces dr::mp::__detail::allocator (include/dr/mp/allocator.hpp:14-33,
+ * sycl::malloc_device under mp::init(queue, usm::alloc::device)) and
+ * __detail::sycl_copy (include/dr/mp/sycl_support.hpp:51-53), so host code
+ * above this ABI needs no CUDA headers.  kind: 0 host->device, 1 device->host,
+ * 2 device->device.  drb_memcpy is asynchronous on `stream` (host memory must
+ * stay valid until the stream is synchronised). */
+drb_status drb_malloc(void **ptr, size_t bytes);
+drb_status drb_free(void *ptr);
+drb_status drb_memcpy(void *dst, const void *src, size_t bytes, int kind,
+                      void *stream);
+drb_status drb_memset(void *dst, int value, size_t bytes, void *stream);
+drb_status drb_stream_synchronize(void *stream);
 
 /* ---- misc ----------------------------------------------------------------- */
 
