@@ -174,7 +174,9 @@ def run_reference(args):
 
 
 def workload_config(alpha, nnz):
-    return {"workload": "csr_powerlaw_16M_fp32", "rows": M, "cols": N_COLS, "nnz": nnz,
+    name = ("csr_powerlaw_16M_fp32" if (M, N_COLS) == (16_777_216, 16_777_216)
+            else f"csr_powerlaw_{M}x{N_COLS}_fp32")
+    return {"workload": name, "rows": M, "cols": N_COLS, "nnz": nnz,
             "row_len": f"zipf alpha={alpha:.4f} on [1,{ZIPF_HI}] (mean {ZIPF_MEAN})",
             "index": "int32", "values": "U(-1,1) fp32", "x": "U(-1,1) fp32", "k": 1,
             "l2": "inputs (2.9 GB) larger than L2; no flush", "parallelism": "replicas"}
@@ -378,7 +380,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows", type=int, default=M,
+                    help="rows of the power-law matrix (profiling a smaller case)")
+    ap.add_argument("--cols", type=int, default=N_COLS,
+                    help="columns (keep 16777216 to keep the 64 MB x footprint)")
     args = ap.parse_args()
+    globals()["M"] = args.rows
+    globals()["N_COLS"] = args.cols
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
