@@ -618,6 +618,22 @@ drb_status drb_dense_gemv(int64_t m, int64_t n, const void *Am, int64_t lda,
                       static_cast<cudaStream_t>(stream));
 }
 
+drb_status drb_dot_noalloc(int64_t n, const void *a, const void *b,
+                           drb_dtype dtype, double *out, void *stream) {
+  clear_error();
+  if (n < 0 || !out || (n > 0 && (!a || !b)))
+    return invalid("NULL pointer or negative n");
+  if (n > dot_noalloc_max_n()) {
+    set_error("invalid argument: drb_dot_noalloc: n = %lld exceeds the maximum %lld "
+              "elements that its static scratch covers; use drb_dot",
+              (long long)n, (long long)dot_noalloc_max_n());
+    return DRB_ERR_INVALID_ARG;
+  }
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  return dot_noalloc_launch(n, a, b, dtype, out, static_cast<cudaStream_t>(stream));
+}
+
 drb_status drb_malloc(void **ptr, size_t bytes) {
   clear_error();
   if (!ptr)

@@ -10,6 +10,9 @@
 // (include/dr/mp/algorithms/reduce.hpp:58-107,
 // benchmarks/gbench/common/dot_product.cpp:33-52) with one launch and a
 // fixed summation order.
+#include <algorithm>
+#include <mutex>
+
 #include "drb_internal.cuh"
 
 namespace drb {
@@ -234,7 +237,72 @@ __global__ void __launch_bounds__(kDotNT)
   }
 }
 
+// ---- dot without allocation --------------------------------------------------
+// Scratch of drb_dot_noalloc: one f64 partial per CTA plus the ticket, in a
+// file-scope device array that every GPU loading the library keeps until
+// process exit (kNoAllocSlots * 8 bytes + 256 = 512.25 KiB).  Each CTA covers
+// kNoAllocBlock elements, so the largest vector is kNoAllocSlots *
+// kNoAllocBlock elements.
+constexpr int kNoAllocBlock = kDotNT * 32;   // 8192 elements per CTA
+constexpr int kNoAllocSlots = 65536;         // partials (one per CTA)
+constexpr int64_t kNoAllocMaxN = (int64_t)kNoAllocBlock * kNoAllocSlots; // 2^29
+static __device__ __align__(256) double g_dot_noalloc_scratch[kNoAllocSlots + 32];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[64];
+
+// Device address of the scratch array on the current device.  Host code only
+// sees a host-side stand-in under that name, so the address is looked up once
+// per device with that device current and cached.
+drb_status noalloc_scratch(double **out) {
+  int dev = 0;
+  DRB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("drb_dot_noalloc: device %d out of range", dev);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    DRB_CUDA_TRY(cudaGetSymbolAddress(&p, g_dot_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<double *>(g_noalloc_addr[dev]);
+  return DRB_OK;
+}
+
 } // namespace
+
+int64_t dot_noalloc_max_n() { return kNoAllocMaxN; }
+
+drb_status dot_noalloc_launch(int64_t n, const void *a, const void *b,
+                              drb_dtype dt, double *out, cudaStream_t s) {
+  if (n > kNoAllocMaxN) {
+    set_error("drb_dot_noalloc: n = %lld exceeds the maximum %lld elements that its "
+              "static scratch covers; use drb_dot",
+              (long long)n, (long long)kNoAllocMaxN);
+    return DRB_ERR_INVALID_ARG;
+  }
+  if (dt != DRB_F32 && dt != DRB_F64) {
+    set_error("drb_dot_noalloc: dtype %d not supported", (int)dt);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  double *scratch = nullptr;
+  DRB_TRY(noalloc_scratch(&scratch));
+  int *ticket = reinterpret_cast<int *>(scratch + kNoAllocSlots);
+  // the array keeps the previous call's contents: the ticket must start at 0
+  DRB_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(int), s));
+  const int64_t grid = std::max<int64_t>(1, (n + kNoAllocBlock - 1) / kNoAllocBlock);
+  if (dt == DRB_F32)
+    dot_kernel<float><<<(unsigned)grid, kDotNT, 0, s>>>(
+        n, (const float *)a, (const float *)b, scratch, ticket, out);
+  else
+    dot_kernel<double><<<(unsigned)grid, kDotNT, 0, s>>>(
+        n, (const double *)a, (const double *)b, scratch, ticket, out);
+  note_launch();
+  DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
+}
 
 drb_status dense_launch(int64_t m, int64_t n, const void *A, int64_t lda,
                         const void *x, void *y, int64_t k, drb_layout layout,

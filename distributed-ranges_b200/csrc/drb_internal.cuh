@@ -178,6 +178,9 @@ drb_status dense_launch(int64_t m, int64_t n, const void *A, int64_t lda,
                         drb_dtype dt, cudaStream_t s);
 drb_status dot_launch(int64_t n, const void *a, const void *b, drb_dtype dt,
                       double *out, cudaStream_t s);
+drb_status dot_noalloc_launch(int64_t n, const void *a, const void *b,
+                              drb_dtype dt, double *out, cudaStream_t s);
+int64_t dot_noalloc_max_n();
 drb_status convert_launch(const void *in, int in_bytes, void *out,
                           int out_bytes, int64_t count, bool to_bf16,
                           cudaStream_t s);

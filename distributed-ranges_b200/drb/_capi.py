@@ -84,6 +84,7 @@ DRB_SYMBOLS = [
     ("drb_csr_update_values", _st, [_vp, _vp, _vp]),
     ("drb_dense_gemv", _st, [_i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _i32, _vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
+    ("drb_dot_noalloc", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_malloc", _st, [C.POINTER(_vp), C.c_size_t]),
     ("drb_free", _st, [_vp]),
     ("drb_memcpy", _st, [_vp, _vp, C.c_size_t, _i32, _vp]),

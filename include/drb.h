@@ -180,6 +180,24 @@ drb_status drb_dense_gemv(int64_t m, int64_t n, const void *A, int64_t lda,
 drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
                    double *out, void *stream);
 
+/* drb_dot without any allocation.  No counterpart in the reference: it exists
+ * for callers that must not allocate device memory during the call -- code
+ * running under a fixed memory budget, inside a caller's own allocator or
+ * memory-pool callback, or on a stream whose allocations the caller has to
+ * account for.  drb_dot takes its per-call scratch (one partial per CTA and a
+ * completion ticket) from cudaMallocAsync; this variant takes it from a static
+ * device array of 512 KiB that the library reserves on every GPU that loads
+ * it, until process exit.  Limit: n <= 2^29 (536,870,912) elements; larger n
+ * returns DRB_ERR_INVALID_ARG (use drb_dot).  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current, so make that first call before any stream capture.  Every
+ * call shares the one array: calls that overlap on the GPU (different
+ * streams, or different host threads) race and may return wrong sums, so
+ * serialise them.  Same result contract as drb_dot (f64, deterministic for a
+ * given n), though its partial sums are grouped differently. */
+drb_status drb_dot_noalloc(int64_t n, const void *a, const void *b,
+                           drb_dtype dtype, double *out, void *stream);
+
 /* ---- device memory (the reference's allocator and sycl_copy) --------------
  * Replaces dr::mp::__detail::allocator (include/dr/mp/allocator.hpp:14-33,
  * sycl::malloc_device under mp::init(queue, usm::alloc::device)) and
