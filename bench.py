@@ -218,6 +218,7 @@ def run_ours(args):
                                      distr=mp.csr_row_distribution,
                                      adjoint=not args.no_extra, autotune=True)
     vb, cb, rb = A.storage_bytes()
+    variant = A.variant()
     bytes_ = alg_bytes(M, N_COLS, nnz, vb, cb, rb, 4, 4)
     xd = torch.from_numpy(x).cuda()
     yd = torch.empty(M, dtype=torch.float32, device="cuda")
@@ -293,8 +294,14 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
-                         "traffic": profiled_traffic("spmv_rowblocks_powerlaw16M_fp32"),
-                         "kernel": "spmv_rowblocks<float,int,int>",
+                         "traffic": (profiled_traffic("spmv_warp_powerlaw16M_fp32")
+                                     if (M, N_COLS) == (16_777_216, 16_777_216) else None),
+                         "kernel": "spmv_warp<float,int,int,%d,%d>" % (variant & ~1, variant & 1),
+                         "gather_ceiling": {
+                             "what": "random x gathers: ~1 L1->crossbar request per SM per "
+                                     "clock (288 G/s measured on this B200)",
+                             "ceiling_GBps": round(288e9 * bytes_ / nnz / 1e9, 1),
+                             "frac": round(achieved / (288e9 * bytes_ / nnz / 1e9), 4)},
                          "alg_bytes_per_launch": bytes_,
                          "kernel_ms": round(kern_ms, 4)},
             "cpu_baseline": cpu,
