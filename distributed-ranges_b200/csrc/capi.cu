@@ -506,7 +506,9 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
     return DRB_OK;
   DeviceGuard g(A->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t xb = (size_t)(A->storage == DRB_BF16 ? 2 : dtype_bytes(A->storage));
+  const size_t xb = (size_t)(A->storage == DRB_BF16
+                                 ? ((A->flags & DRB_FLAG_BF16_X_F32) ? 4 : 2)
+                                 : dtype_bytes(A->storage));
   const size_t yb = (size_t)(A->storage == DRB_BF16 ? 4 : dtype_bytes(A->storage));
   DRB_TRY(A->xh_dev.ensure(xb * A->n * k));
   DRB_TRY(A->yh_dev.ensure(yb * A->m * k));

@@ -540,7 +540,7 @@ drb_status build_plan(Plan &plan, int64_t m, const void *rowptr_host,
 
 drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
                        drb_layout layout, cudaStream_t s) {
-  if (k == 1 && (A.storage == DRB_F32 || A.storage == DRB_F64))
+  if (k == 1)
     return spmv_pipe_launch(A, x, y, s);
   switch (A.storage) {
   case DRB_F32:

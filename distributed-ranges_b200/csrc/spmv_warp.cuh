@@ -1,0 +1,486 @@
+// spmv_warp.cuh -- persistent warp-granular CSR SpMV (one right-hand side).
+//
+// The matrix is cut once (build_pipe_plan, spmv_warp.cu) into work items of at
+// most TILE nonzeros counted from a 16-byte aligned start: up to kRows whole
+// short rows, or one fixed-size chunk of a long row.  Every warp of the grid
+// owns the items w, w + W, w + 2W, ... (W = warps in the grid) and runs them
+// with no CTA-wide barrier, so warps progress independently.
+//
+// For its current item every lane holds TILE/32 nonzeros in registers
+// (16-byte vector loads of colind and values, evict-first L2 policy), gathers
+// x for all of them at once (evict-last L2 policy keeps x resident), stores
+// the products to its warp's shared-memory slice, and immediately reloads the
+// registers with its next item; the current item's rows are then summed from
+// shared memory while the next item's loads are in flight.  With SKEW the
+// products are stored skewed (element q at q + q/32) so lanes that sum
+// different rows hit different banks; rows are summed by 1..32 lanes each.
+//
+// Storage and accumulation types: V is the stored element type of values and
+// x (float, double, or bfloat16 bits in uint16_t); products and sums use
+// Acc = float for float/bf16 and double for double; y has type Acc.  With
+// COMP the sums are two-sum compensated (a running sum plus the rounding
+// error of every addition, combined at the end), so a bf16 x bf16 product,
+// exact in fp32, reaches y with only the final rounding.
+//
+// On B200 the random x gathers are bounded by the SM's L1-to-crossbar request
+// rate (about one request per SM per clock); the design keeps many gathers in
+// flight per warp and as many warps as registers allow.
+//
+// A chunked long row writes one partial per chunk; the warp that completes
+// the last chunk (ticket counter) adds the partials in chunk order.  Every sum
+// has a fixed order, so results are deterministic.
+#pragma once
+
+#include <algorithm>
+
+#include "drb_internal.cuh"
+
+namespace drb::warpk {
+
+constexpr int kRows = 64; // rows of a whole-row item (<= 64: three rowptr regs)
+constexpr int kWarps = 8; // warps per CTA
+constexpr int kThreads = kWarps * 32;
+
+template <class V> struct AccOf {
+  using type = float;
+};
+template <> struct AccOf<double> {
+  using type = double;
+};
+
+__device__ __forceinline__ float to_acc(float v) { return v; }
+__device__ __forceinline__ double to_acc(double v) { return v; }
+__device__ __forceinline__ float to_acc(uint16_t v) {
+  return __uint_as_float(((uint32_t)v) << 16);
+}
+
+__device__ __forceinline__ float ld_x(const float *p, uint64_t pol) {
+  return ptx::ld_keep(p, pol);
+}
+__device__ __forceinline__ double ld_x(const double *p, uint64_t pol) {
+  return ptx::ld_keep(p, pol);
+}
+__device__ __forceinline__ float ld_x(const uint16_t *p, uint64_t pol) {
+  return ptx::ld_keep(reinterpret_cast<const __nv_bfloat16 *>(p), pol);
+}
+
+template <class T> union Vec16 {
+  uint4 u;
+  T t[16 / sizeof(T)];
+};
+
+template <class T, int G>
+__device__ __forceinline__ void ld_group(const T *p, T (&out)[G], uint64_t pol) {
+  constexpr int PER = 16 / sizeof(T);
+#pragma unroll
+  for (int v = 0; v < G / PER; v++) {
+    Vec16<T> r;
+    r.u = ptx::ld_stream16(p + v * PER, pol);
+#pragma unroll
+    for (int i = 0; i < PER; i++)
+      out[v * PER + i] = r.t[i];
+  }
+}
+
+template <class T> __device__ __forceinline__ T wsum(T v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// Knuth's two-sum: s + e == a + b exactly, s = fl(a + b).
+template <class T> __device__ __forceinline__ void two_sum(T a, T b, T &s, T &e) {
+  s = a + b;
+  const T bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// Compensated accumulator (running sum and error term).
+template <class T> struct CSum {
+  T s = 0, c = 0;
+  __device__ __forceinline__ void add(T x) {
+    T e;
+    two_sum(s, x, s, e);
+    c += e;
+  }
+  __device__ __forceinline__ void merge(T s2, T c2) {
+    T e;
+    two_sum(s, s2, s, e);
+    c += c2 + e;
+  }
+  __device__ __forceinline__ T value() const { return s + c; }
+};
+
+__device__ __forceinline__ Item load_item(const Item *items, int64_t i) {
+  const int4 *p = reinterpret_cast<const int4 *>(items + i);
+  const int4 a = __ldg(p), b = __ldg(p + 1);
+  Item d;
+  d.p0 = (int64_t)(((uint64_t)(uint32_t)a.y << 32) | (uint32_t)a.x);
+  d.len = a.z;
+  d.r0 = a.w;
+  d.nrows = b.x;
+  d.chunk = b.y;
+  d.pad0 = d.pad1 = 0;
+  return d;
+}
+
+__device__ __forceinline__ int skew(int q) { return q + (q >> 5); }
+
+// Fused ||A x - b||^2: whole rows add into a per-CTA partial; a chunked row's
+// square goes to its own slot because which warp finishes it varies run to
+// run.  The last CTA sums partials[0..grid) then rowres[0..nsplit) in order.
+struct WarpResid {
+  const void *b = nullptr;
+  double *partials = nullptr;
+  double *rowres = nullptr;
+  int64_t nsplit = 0;
+  int *ticket = nullptr;
+  double *out = nullptr;
+};
+
+template <class V, class CI, int TILE> struct Slot {
+  static constexpr int G = 16 / (sizeof(V) < sizeof(CI) ? sizeof(V) : sizeof(CI));
+  static constexpr int NG = TILE / (G * 32);
+  static_assert(NG >= 1 && TILE % (G * 32) == 0, "tile/group");
+  V v[NG][G];
+  CI c[NG][G];
+  Item d;
+  int64_t a0;
+  int rp0, rp1, rp2;
+  bool valid;
+};
+
+template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP> struct Kern {
+  using Acc = typename AccOf<V>::type;
+  using S = Slot<V, CI, TILE>;
+  static constexpr int G = S::G, NG = S::NG;
+  const RI *__restrict__ rowptr;
+  const CI *__restrict__ colind;
+  const V *__restrict__ vals;
+  const XT *__restrict__ x;
+  Acc *__restrict__ y;
+  const Item *__restrict__ items;
+  int64_t nitems;
+  const Chunk *__restrict__ chunks;
+  Acc *partials;
+  int *counters;
+  uint64_t pol_s, pol_x;
+  int lane;
+
+  __device__ __forceinline__ void fetch(S &sl, int64_t i) {
+    sl.valid = i < nitems;
+    if (!sl.valid)
+      return;
+    sl.d = load_item(items, i);
+    sl.a0 = sl.d.p0 & ~(int64_t)(G - 1);
+    const int ng = (int)((sl.d.p0 + sl.d.len - sl.a0 + G - 1) / G);
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+      if (g < ng) {
+        ld_group<V, G>(vals + sl.a0 + (int64_t)g * G, sl.v[j], pol_s);
+        ld_group<CI, G>(colind + sl.a0 + (int64_t)g * G, sl.c[j], pol_s);
+      }
+    }
+    if (sl.d.nrows > 0) {
+      // rowptr[r0 .. r0 + nrows] relative to a0 (nrows <= kRows = 64)
+      const int64_t r0 = sl.d.r0;
+      if (lane <= sl.d.nrows)
+        sl.rp0 = (int)((int64_t)rowptr[r0 + lane] - sl.a0);
+      if (lane + 32 <= sl.d.nrows)
+        sl.rp1 = (int)((int64_t)rowptr[r0 + lane + 32] - sl.a0);
+      if (lane == 0 && 64 <= sl.d.nrows)
+        sl.rp2 = (int)((int64_t)rowptr[r0 + 64] - sl.a0);
+    }
+  }
+
+  // Reduce over a group of `tpr` lanes (segments of a warp), plain or
+  // compensated.  The result is valid in the group's first lane.
+  __device__ __forceinline__ Acc group_sum(Acc s, Acc c, int tpr) {
+    if (!COMP) {
+      for (int o = tpr >> 1; o > 0; o >>= 1)
+        s += __shfl_down_sync(0xffffffffu, s, o, tpr);
+      return s;
+    }
+    CSum<Acc> t;
+    t.s = s;
+    t.c = c;
+    for (int o = tpr >> 1; o > 0; o >>= 1) {
+      const Acc s2 = __shfl_down_sync(0xffffffffu, t.s, o, tpr);
+      const Acc c2 = __shfl_down_sync(0xffffffffu, t.c, o, tpr);
+      t.merge(s2, c2);
+    }
+    return t.value();
+  }
+
+  // Runs the item in `sl` and refills the slot with item `refill`.
+  template <bool RESID>
+  __device__ __forceinline__ void process(S &sl, int64_t refill, Acc *prod, int *srp,
+                                          const Acc *bvec, double &r2, double *rowres) {
+    const Item cur = sl.d;
+    const int off = (int)(cur.p0 - sl.a0), end = off + cur.len;
+    const int ng = (end + G - 1) / G;
+    Acc xg[NG][G];
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        const int q = g * G + i;
+        xg[j][i] = (g < ng && q >= off && q < end) ? ld_x(x + sl.c[j][i], pol_x) : Acc(0);
+      }
+    }
+    if (cur.nrows == 0) {
+      // one chunk of a long row: sum in registers, no shared memory
+      CSum<Acc> acc;
+#pragma unroll
+      for (int j = 0; j < NG; j++) {
+        const int g = lane + 32 * j;
+#pragma unroll
+        for (int i = 0; i < G; i++) {
+          const int q = g * G + i;
+          if (g < ng && q >= off && q < end) {
+            const Acc p = to_acc(sl.v[j][i]) * xg[j][i];
+            if (COMP)
+              acc.add(p);
+            else
+              acc.s += p;
+          }
+        }
+      }
+      fetch(sl, refill);
+      const Acc tot = group_sum(acc.s, acc.c, 32);
+      if (lane == 0)
+        finish_chunk<RESID>(cur, tot, bvec, rowres);
+      return;
+    }
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+      if (g < ng) {
+        if (SKEW) {
+#pragma unroll
+          for (int i = 0; i < G; i++)
+            prod[skew(g * G + i)] = to_acc(sl.v[j][i]) * xg[j][i];
+        } else {
+          constexpr int PER = 16 / sizeof(Acc);
+#pragma unroll
+          for (int h = 0; h < G / PER; h++) {
+            Vec16<Acc> w;
+#pragma unroll
+            for (int i = 0; i < PER; i++)
+              w.t[i] = to_acc(sl.v[j][h * PER + i]) * xg[j][h * PER + i];
+            *reinterpret_cast<uint4 *>(prod + g * G + h * PER) = w.u;
+          }
+        }
+      }
+    }
+    if (lane <= cur.nrows)
+      srp[lane] = sl.rp0;
+    if (lane + 32 <= cur.nrows)
+      srp[lane + 32] = sl.rp1;
+    if (lane == 0 && 64 <= cur.nrows)
+      srp[64] = sl.rp2;
+    __syncwarp();
+    fetch(sl, refill); // the slot's registers are free again
+
+    const int nrows = cur.nrows;
+    int tpr = 1;
+    while (tpr < 32 && tpr * 2 * nrows <= 32)
+      tpr <<= 1;
+    const int groups = 32 / tpr, gid = lane / tpr, gl = lane & (tpr - 1);
+    for (int base = 0; base < nrows; base += groups) {
+      const int r = base + gid;
+      CSum<Acc> acc;
+      if (r < nrows) {
+        const int b = srp[r], e = srp[r + 1];
+        for (int q = b + gl; q < e; q += tpr) {
+          const Acc p = prod[SKEW ? skew(q) : q];
+          if (COMP)
+            acc.add(p);
+          else
+            acc.s += p;
+        }
+      }
+      const Acc tot = group_sum(acc.s, acc.c, tpr);
+      if (r < nrows && gl == 0) {
+        y[cur.r0 + r] = tot;
+        if (RESID) {
+          const double dd = (double)tot - (double)bvec[cur.r0 + r];
+          r2 += dd * dd;
+        }
+      }
+    }
+    __syncwarp(); // the shared slice is rewritten by the next item
+  }
+
+  // Lane 0 after a chunk: publish the partial; the last chunk of the row
+  // adds all partials in chunk order and writes y.
+  template <bool RESID>
+  __device__ __forceinline__ void finish_chunk(const Item &cur, Acc tot, const Acc *bvec,
+                                               double *rowres) {
+    const Chunk ch = chunks[cur.chunk];
+    partials[cur.chunk] = tot;
+    __threadfence();
+    const int t = atomicAdd(&counters[ch.counter], 1);
+    if (t == ch.count - 1) {
+      __threadfence();
+      CSum<Acc> sum;
+      for (int i = 0; i < ch.count; i++) {
+        const Acc p = *(volatile Acc *)&partials[ch.first + i];
+        if (COMP)
+          sum.add(p);
+        else
+          sum.s += p;
+      }
+      const Acc v = sum.value();
+      y[ch.row] = v;
+      counters[ch.counter] = 0; // re-armed for the next launch
+      if (RESID) {
+        const double dd = (double)v - (double)bvec[ch.row];
+        rowres[ch.counter] = dd * dd;
+      }
+    }
+  }
+};
+
+template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP>
+__global__ void __launch_bounds__(kThreads)
+    spmv_warp(const RI *__restrict__ rowptr, const CI *__restrict__ colind,
+              const V *__restrict__ vals, const XT *__restrict__ x,
+              typename AccOf<V>::type *__restrict__ y, const Item *__restrict__ items,
+              int64_t nitems, const Chunk *__restrict__ chunks,
+              typename AccOf<V>::type *partials, int *counters, WarpResid ra) {
+  using Acc = typename AccOf<V>::type;
+  __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
+  __shared__ int s_rp[kWarps][kRows + 1];
+  __shared__ double s_red[kWarps];
+  __shared__ int s_last;
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  Kern<V, XT, CI, RI, TILE, SKEW, COMP> K{rowptr, colind, vals, x, y, items, nitems,
+                                      chunks, partials, counters,
+                                      ptx::policy_evict_first(), ptx::policy_evict_last(),
+                                      lane};
+  const int64_t nw = (int64_t)gridDim.x * kWarps;
+  int64_t it = (int64_t)blockIdx.x * kWarps + warp;
+  const Acc *bvec = static_cast<const Acc *>(ra.b);
+  double r2 = 0.0;
+  Acc *prod = s_prod[warp];
+  int *srp = s_rp[warp];
+
+  Slot<V, CI, TILE> A;
+  K.fetch(A, it);
+  while (A.valid) {
+    K.template process<RESID>(A, it + nw, prod, srp, bvec, r2, ra.rowres);
+    it += nw;
+  }
+
+  if (RESID) {
+    const double t = wsum(r2);
+    if (lane == 0)
+      s_red[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double cta = 0.0;
+      for (int w = 0; w < kWarps; w++)
+        cta += s_red[w];
+      ra.partials[blockIdx.x] = cta;
+      __threadfence();
+      s_last = atomicAdd(ra.ticket, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+      // The last CTA adds the per-CTA partials and the chunked-row slots with
+      // all its threads: fixed strided assignment, then a fixed-order tree.
+      __threadfence();
+      const int64_t total = (int64_t)gridDim.x + ra.nsplit;
+      double sum = 0.0;
+      for (int64_t i = threadIdx.x; i < total; i += kThreads)
+        sum += i < gridDim.x ? __ldcg(&ra.partials[i]) : __ldcg(&ra.rowres[i - gridDim.x]);
+      sum = wsum(sum);
+      if (lane == 0)
+        s_red[warp] = sum;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t2 = 0.0;
+        for (int w = 0; w < kWarps; w++)
+          t2 += s_red[w];
+        *ra.out = t2;
+        *ra.ticket = 0;
+      }
+    }
+  }
+}
+
+struct Shape {
+  int grid = 0;
+  bool ready = false;
+};
+
+template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP>
+drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
+                       cudaStream_t s) {
+  using Acc = typename AccOf<V>::type;
+  PipePlan &P = A.pipe;
+  static Shape shape[64];
+  auto kern = spmv_warp<V, XT, CI, RI, TILE, SKEW, RESID, COMP>;
+  const int dev = A.device < 64 ? A.device : 0;
+  if (!shape[dev].ready) {
+    int occ = 0, sms = 0;
+    DRB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, 0));
+    DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
+    shape[dev].grid = std::max(1, occ) * sms;
+    shape[dev].ready = true;
+  }
+  const int64_t need = (P.nitems + kWarps - 1) / kWarps;
+  const int grid = (int)std::min<int64_t>(shape[dev].grid, need);
+  WarpResid r{};
+  if (ra)
+    r = *ra;
+  kern<<<grid, kThreads, 0, s>>>(A.rowptr.as<RI>(), A.colind.as<CI>(), A.vals.as<V>(),
+                                 static_cast<const XT *>(x), static_cast<Acc *>(y),
+                                 P.items.as<Item>(), P.nitems, P.chunks.as<Chunk>(),
+                                 P.partials.as<Acc>(), P.counters.as<int>(), r);
+  note_launch();
+  DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
+}
+
+template <class V, class XT, class CI, class RI, bool RESID, bool COMP>
+drb_status launch_variant(Csr &A, const void *x, void *y, const WarpResid *ra,
+                          cudaStream_t s) {
+  if (A.pipe.nitems == 0)
+    return DRB_OK;
+  const bool sk = A.pipe.skew;
+  if (A.pipe.tile == 512)
+    return sk ? launch_tile<V, XT, CI, RI, 512, true, RESID, COMP>(A, x, y, ra, s)
+              : launch_tile<V, XT, CI, RI, 512, false, RESID, COMP>(A, x, y, ra, s);
+  return sk ? launch_tile<V, XT, CI, RI, 256, true, RESID, COMP>(A, x, y, ra, s)
+            : launch_tile<V, XT, CI, RI, 256, false, RESID, COMP>(A, x, y, ra, s);
+}
+
+// Dispatch on the stored index widths.
+template <class V, class XT, bool RESID, bool COMP>
+drb_status launch_typed(Csr &A, const void *x, void *y, const WarpResid *ra,
+                        cudaStream_t s) {
+  if (A.cbytes == 4 && A.rbytes == 4)
+    return launch_variant<V, XT, int32_t, int32_t, RESID, COMP>(A, x, y, ra, s);
+  if (A.cbytes == 4 && A.rbytes == 8)
+    return launch_variant<V, XT, int32_t, int64_t, RESID, COMP>(A, x, y, ra, s);
+  if (A.cbytes == 8 && A.rbytes == 4)
+    return launch_variant<V, XT, int64_t, int32_t, RESID, COMP>(A, x, y, ra, s);
+  return launch_variant<V, XT, int64_t, int64_t, RESID, COMP>(A, x, y, ra, s);
+}
+
+} // namespace drb::warpk
+
+namespace drb {
+// Per storage type (defined in spmv_warp_f32.cu / _f64.cu / _bf16.cu).
+drb_status warp_launch_f32(Csr &A, const void *x, void *y, const warpk::WarpResid *ra,
+                           bool comp, cudaStream_t s);
+drb_status warp_launch_f64(Csr &A, const void *x, void *y, const warpk::WarpResid *ra,
+                           cudaStream_t s);
+drb_status warp_launch_bf16(Csr &A, const void *x, void *y, bool x_f32, cudaStream_t s);
+} // namespace drb

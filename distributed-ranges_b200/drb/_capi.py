@@ -41,6 +41,7 @@ DRB_FLAG_SKIP_VALIDATE = 0x4
 DRB_FLAG_ADJOINT = 0x8
 DRB_FLAG_COMPENSATED = 0x10
 DRB_FLAG_AUTOTUNE = 0x20
+DRB_FLAG_BF16_X_F32 = 0x40
 
 STATUS_NAMES = {
     0: "DRB_OK", 1: "DRB_ERR_INVALID_ARG", 2: "DRB_ERR_BAD_CSR",

@@ -190,7 +190,7 @@ class distributed_sparse_matrix:
                  *, distr=csr_eq_distribution, nsegments: int = 1,
                  storage=None, adjoint: bool = False,
                  keep_index64: bool = False, autotune: bool = False,
-                 stream=None):
+                 compensated: bool = False, x_dtype=None, stream=None):
         if root != 0:
             raise ValueError(f"root {root} is not a rank: one process owns the GPU")
         self._h = C.c_void_p(0)
@@ -218,6 +218,10 @@ class distributed_sparse_matrix:
             flags |= capi.DRB_FLAG_KEEP_INDEX64
         if autotune:
             flags |= capi.DRB_FLAG_AUTOTUNE
+        if compensated:
+            flags |= capi.DRB_FLAG_COMPENSATED
+        if st == capi.DRB_BF16 and x_dtype == torch.float32:
+            flags |= capi.DRB_FLAG_BF16_X_F32
         h = C.c_void_p()
         check(capi.lib.drb_csr_create(
             C.byref(h), m, n, nnz, _ptr(rowptr), _ptr(colind), _ptr(values),
@@ -229,6 +233,9 @@ class distributed_sparse_matrix:
         self.value_dtype = _STORAGE_TORCH[vt]
         self.storage_dtype = _STORAGE_TORCH[st]
         self.compute_dtype = torch.float32 if st == capi.DRB_BF16 else self.storage_dtype
+        # element type of x: the storage type, except bf16 values with f32 x
+        self.x_dtype = (torch.float32 if flags & capi.DRB_FLAG_BF16_X_F32
+                        else self.storage_dtype)
         self._ybuf: dict = {}
 
     # ---- reference accessors ----
@@ -446,8 +453,8 @@ def gemv(*args, stream=None) -> None:
         if b.size() != n:
             raise ValueError(f"x has {b.size()} elements, expected {n}")
     x = b.broadcasted_data()
-    if x.dtype != a.compute_dtype and not (a.storage_dtype == torch.bfloat16 and x.dtype == torch.bfloat16):
-        x = x.to(a.storage_dtype)
+    if x.dtype != a.x_dtype:
+        x = x.to(a.x_dtype)
     a.local_gemv_and_collect(root, res, x, width, stream=stream)
 
 

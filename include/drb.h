@@ -75,6 +75,7 @@ typedef enum { DRB_PART_ROW = 0, DRB_PART_EQ = 1 } drb_partition;
 #define DRB_FLAG_ADJOINT 0x8u        /* build the CSC plan for gemv_backward */
 #define DRB_FLAG_COMPENSATED 0x10u   /* two-sum compensated FP32 row sums    */
 #define DRB_FLAG_AUTOTUNE 0x20u      /* run drb_csr_autotune at create       */
+#define DRB_FLAG_BF16_X_F32 0x40u    /* BF16 storage: x stays f32 (not bf16)  */
 
 typedef struct drb_csr_matrix *drb_csr_t;
 
@@ -123,8 +124,10 @@ drb_status drb_csr_get_entries(drb_csr_t A, int64_t offset, int64_t count,
 /* ---- the hot call ------------------------------------------------------- */
 
 /* y = A * x for k right-hand sides, device pointers.  Element types: x and y
- * have the storage type, except BF16 storage: x bf16, y f32.  y is
- * overwritten (the reference zero-fills its partial result first). */
+ * have the storage type, except BF16 storage: x bf16 (f32 with
+ * DRB_FLAG_BF16_X_F32), y f32, products exact in f32 and summed with two-sum
+ * compensation.  BF16 storage takes k = 1.  y is overwritten (the reference
+ * zero-fills its partial result first). */
 drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
                         drb_layout layout, void *stream);
 
