@@ -1,0 +1,1069 @@
+// batch.cu -- batched CSR SpMM: Y_i = A_i X_i over many handles in one
+// persistent launch, captured once in a CUDA graph.
+//
+// No reference counterpart: the reference multiplies one matrix per
+// dr::mp::gemv call (include/dr/mp/algorithms/matrix/gemv.hpp:29-39, k
+// right-hand sides as a broadcasted_slim_matrix, column-major).
+//
+// Work list.  Every matrix is cut into items of whole rows with at most CAP
+// nonzeros and RMAX rows; a row longer than CAP is an item of its own (a
+// "long row").  An item is 16 bytes {matrix, first row, rows | nnz << 8,
+// first nonzero}; the items of all matrices form one list, and with more
+// right-hand sides than one block holds, (item, block) pairs are the units.
+// Warp w of the persistent grid runs units w, w + W, w + 2W, ... (W = warps in
+// the grid): units hold at most CAP nonzeros, so the static split balances,
+// and no warp waits on another (no spin anywhere).
+//
+// Random gathers of X rows bound this kernel.  Every warp runs a software
+// pipeline over its units: while unit t computes, the column indices,
+// values and row offsets of unit t+1 stream into shared memory (16-byte
+// cp.async chunks, no registers held), and the item record of unit t+2 is
+// read.  For unit t, groups of G slots (a slot = KP lanes, each lane VEC
+// consecutive right-hand sides) share a row and R = S/G rows run at once; a
+// lane keeps four 16-byte X gathers in flight (read-only path; k = 16 fp32 is
+// one 64-byte row per nonzero), a group's partial sums meet in a fixed
+// xor-shuffle tree, and the row sums go to a shared tile that the warp
+// stores to Y coalesced, in either layout.  A long row is staged CAP
+// nonzeros at a time and summed by all slots.  Every output element is
+// summed in a fixed order: results are deterministic and, for a given G,
+// independent of CAP for rows of at most 128 nonzeros.
+//
+// X in column-major layout (the reference's slim matrix) is first packed by a
+// batched tiled transpose, in the same graph, into a row-major copy whose
+// rows are padded to a multiple of VEC.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "drb_internal.cuh"
+
+namespace drb {
+namespace {
+
+constexpr int kWarps = 8; // warps per CTA
+constexpr int kYBudget = 4096; // bytes of a warp's output tile
+constexpr int kRmax = 32;      // rows per item
+constexpr int kNumCaps = 3;
+constexpr int kCaps[kNumCaps] = {128, 256, 512};
+
+struct BMat { // one per matrix of the batch (64 bytes)
+  const int32_t *rowptr;
+  const int32_t *colind;
+  const void *vals;
+  const void *x; // row-major, ldx elements per row
+  void *y;
+  int64_t m;
+  int64_t n;
+  int64_t pad;
+};
+static_assert(sizeof(BMat) == 64, "BMat is 64 bytes");
+
+struct PackEnt {
+  const void *src;
+  void *dst;
+  int64_t n;
+  int64_t tile0; // first pack tile of this matrix
+};
+
+struct BArgs {
+  const BMat *mats;
+  const int4 *items;
+  int64_t nunits;
+  int nkb;       // right-hand-side blocks per item
+  int k, ldx;    // right-hand sides; row stride of X (elements)
+  int KP, S, KB; // lanes per slot, slots per warp, RHS per block (KP*VEC)
+  int G;         // slots per row (power of two dividing S)
+  int cap, rmax;
+  int row_major;
+  int warp_bytes;
+  int cols_off, cols_stage, vals_off, vals_stage, rs_off, rs_stage;
+  int y_off;
+};
+
+template <class V> struct AccOf {
+  using type = float;
+};
+template <> struct AccOf<double> {
+  using type = double;
+};
+
+// ---- cp.async (global -> shared, asynchronous, no registers in flight) ----
+// Plain forms: the lanes of one instruction that touch the same line are
+// served by one request.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(uint32_t dst, const void *src) {
+  if constexpr (BYTES == 16) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst),
+                 "l"(src)
+                 : "memory");
+  } else {
+    static_assert(BYTES == 4 || BYTES == 8, "4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst),
+                 "l"(src), "n"(BYTES)
+                 : "memory");
+  }
+}
+__device__ __forceinline__ void cp_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N> __device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+
+__device__ __forceinline__ float to_acc(float v) { return v; }
+__device__ __forceinline__ double to_acc(double v) { return v; }
+__device__ __forceinline__ float to_acc(uint16_t v) {
+  return __uint_as_float(((uint32_t)v) << 16);
+}
+
+
+// VEC consecutive X elements from global memory (read-only path) as raw
+// 32-bit words, decoded to accumulator values only when used, so gathers in
+// flight hold 16 bytes of registers each.
+template <class XT, int VEC> struct XWords {
+  static constexpr int W = VEC * (int)sizeof(XT) / 4;
+  uint32_t w[W];
+};
+template <class XT, int VEC>
+__device__ __forceinline__ void ldg_x(const XT *p, XWords<XT, VEC> &o) {
+  constexpr int W = XWords<XT, VEC>::W;
+  if constexpr (W == 4) {
+    const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p));
+    o.w[0] = u.x, o.w[1] = u.y, o.w[2] = u.z, o.w[3] = u.w;
+  } else if constexpr (W == 2) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+    o.w[0] = u.x, o.w[1] = u.y;
+  } else {
+    o.w[0] = __ldg(reinterpret_cast<const uint32_t *>(p));
+  }
+}
+template <class XT, int VEC, class A>
+__device__ __forceinline__ A x_at(const XWords<XT, VEC> &o, int t) {
+  if constexpr (sizeof(XT) == 4) {
+    return __uint_as_float(o.w[t]);
+  } else if constexpr (sizeof(XT) == 8) {
+    return __hiloint2double((int)o.w[2 * t + 1], (int)o.w[2 * t]);
+  } else {
+    return (t & 1) ? __uint_as_float(o.w[t >> 1] & 0xffff0000u)
+                   : __uint_as_float(o.w[t >> 1] << 16);
+  }
+}
+
+// 32-bit shared-memory loads at explicit shared addresses.
+__device__ __forceinline__ int32_t lds_s32(uint32_t addr) {
+  int32_t v;
+  asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
+  return v;
+}
+template <class V> __device__ __forceinline__ V lds_val(uint32_t addr);
+template <> __device__ __forceinline__ float lds_val<float>(uint32_t addr) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+template <> __device__ __forceinline__ double lds_val<double>(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+  return v;
+}
+template <>
+__device__ __forceinline__ uint16_t lds_val<uint16_t>(uint32_t addr) {
+  uint16_t v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=h"(v) : "r"(addr));
+  return v;
+}
+
+// Copy elements [e0, e0 + cnt) of a 16-byte aligned array to the shared
+// address dst in 16-byte chunks from the aligned element below e0 (the
+// array's allocation is padded, so the last chunk stays inside it).
+template <class T>
+__device__ __forceinline__ void copy16s(uint32_t dst, const T *base,
+                                        int64_t e0, int cnt, int lane) {
+  constexpr int PER = 16 / (int)sizeof(T);
+  const int64_t a0 = e0 & ~(int64_t)(PER - 1);
+  const int nch = (int)((e0 + cnt - a0 + PER - 1) / PER);
+  const T *src = base + a0;
+  for (int c = lane; c < nch; c += 32)
+    cp_async<16>(dst + 16 * c, src + (int64_t)c * PER);
+}
+
+__device__ __forceinline__ int ilog2(int x) { return 31 - __clz(x); }
+__device__ __forceinline__ int clog2(int x) {
+  return ilog2(x) + ((x & (x - 1)) ? 1 : 0);
+}
+
+constexpr int kUnroll = 4; // X gathers in flight per lane
+
+// The nonzeros [b, e) of one row staged at shared addresses colS/valS (byte
+// address of stage element 0), this lane's VEC sums; the lane takes b, b +
+// step, ... with kUnroll gathers in flight.
+template <class V, class XT, int VEC, class A>
+__device__ __forceinline__ void row_sums(uint32_t colS, uint32_t valS, int b,
+                                         int e, const XT *Xl, int ldx,
+                                         int step, A (&acc)[VEC]) {
+  for (int q = b; q < e; q += kUnroll * step) {
+    XWords<XT, VEC> xv[kUnroll];
+    A vv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++) {
+      const int qq = min(q + u * step, e - 1); // in range; extra lanes masked
+      const int32_t col = lds_s32(colS + 4 * qq);
+      const A v = to_acc(lds_val<V>(valS + (uint32_t)sizeof(V) * qq));
+      vv[u] = q + u * step < e ? v : A(0);
+      ldg_x<XT, VEC>(Xl + (int64_t)col * ldx, xv[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++) {
+#pragma unroll
+        for (int t = 0; t < VEC; t++)
+          acc[t] = fma(vv[u], (x_at<XT, VEC, A>(xv[u], t)), acc[t]);
+    }
+  }
+}
+
+template <class V, class XT, int VEC>
+__global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
+  using A = typename AccOf<V>::type;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t wsm = smem_u32(smem) + (uint32_t)(warp * a.warp_bytes);
+  A *ytile = reinterpret_cast<A *>(smem + (size_t)warp * a.warp_bytes + a.y_off);
+  const int KP = a.KP, S = a.S, KB = a.KB, G = a.G, k = a.k, ldx = a.ldx;
+  const int R = S / G;
+  const int slot = lane / KP, jj = lane - slot * KP;
+  const int grp = slot / G, gs = slot - grp * G; // row group, slot in group
+  const bool on = slot < S;
+  const bool row_on = on && grp < R; // slots past R*G idle in short units
+  const int ystride = KB + 1;
+  const int64_t W = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t nunits = a.nunits;
+  const int nkb = a.nkb;
+  constexpr int VOFF_MASK = 16 / (int)sizeof(V) - 1;
+
+  int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  auto item_of = [&](int64_t uu) -> int64_t {
+    return nkb == 1 ? uu : (int64_t)((uint32_t)uu / (uint32_t)nkb);
+  };
+  int4 rec = u < nunits ? __ldg(a.items + item_of(u)) : make_int4(0, 0, 0, 0);
+  int4 rec_n = u + W < nunits ? __ldg(a.items + item_of(u + W))
+                              : make_int4(0, 0, 0, 0);
+
+  // slices (columns, values, row offsets) of a short unit -> stage st
+#define DRB_BATCH_PAIRS(REC, VALID, ST)                                          \
+  do {                                                                         \
+    if ((VALID) && ((REC).z & 0xff) > 0) {                                     \
+      const BMat *bm_ = a.mats + (REC).x;                                      \
+      const int len_ = (REC).z >> 8, nr_ = (REC).z & 0xff;                     \
+      copy16s<int32_t>(wsm + a.cols_off + (ST) * a.cols_stage, bm_->colind,    \
+                       (REC).w, len_, lane);                                   \
+      copy16s<V>(wsm + a.vals_off + (ST) * a.vals_stage,                       \
+                 static_cast<const V *>(bm_->vals), (REC).w, len_, lane);      \
+      copy16s<int32_t>(wsm + a.rs_off + (ST) * a.rs_stage, bm_->rowptr,        \
+                       (REC).y, nr_ + 1, lane);                                \
+    }                                                                          \
+    cp_commit();                                                               \
+  } while (0)
+
+  DRB_BATCH_PAIRS(rec, u < nunits, 0);
+  for (int st = 0; u < nunits; u += W, st ^= 1) {
+    const int4 rec_nn = u + 2 * W < nunits ? __ldg(a.items + item_of(u + 2 * W))
+                                           : make_int4(0, 0, 0, 0);
+    DRB_BATCH_PAIRS(rec_n, u + W < nunits, st ^ 1);
+    cp_wait<1>(); // all but the newest group: the slices of unit u
+    __syncwarp();
+
+    const BMat *bm = a.mats + rec.x;
+    const int jb = nkb == 1 ? 0 : (int)((uint32_t)u % (uint32_t)nkb) * KB;
+    const int c0 = jb + jj * VEC;
+    const bool con = on && c0 < k;
+    const XT *Xl = static_cast<const XT *>(bm->x) + c0;
+    A *Y = static_cast<A *>(bm->y);
+    const int64_t m = bm->m;
+    const int r0 = rec.y, nrows = rec.z & 0xff, p0 = rec.w;
+    const uint32_t colS = wsm + a.cols_off + st * a.cols_stage;
+    const uint32_t valS = wsm + a.vals_off + st * a.vals_stage;
+
+    if (nrows > 0) {
+      // ---- whole rows [r0, r0 + nrows): R rows at a time, G slots each ----
+      const uint32_t colP = colS + 4 * (p0 & 3);
+      const uint32_t valP = valS + (uint32_t)sizeof(V) * (p0 & VOFF_MASK);
+      const uint32_t rsP = wsm + a.rs_off + st * a.rs_stage + 4 * (r0 & 3);
+      for (int i0 = 0; i0 < nrows; i0 += R) {
+        const int i = i0 + grp;
+        A acc[VEC];
+#pragma unroll
+        for (int t = 0; t < VEC; t++)
+          acc[t] = 0;
+        if (con && row_on && i < nrows) {
+          const int b = lds_s32(rsP + 4 * i) - p0, e = lds_s32(rsP + 4 * i + 4) - p0;
+          row_sums<V, XT, VEC, A>(colP, valP, b + gs, e, Xl, ldx, G, acc);
+        }
+        for (int dd = 1; dd < G; dd <<= 1) {
+#pragma unroll
+          for (int t = 0; t < VEC; t++)
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], dd * KP);
+        }
+        if (con && row_on && gs == 0 && i < nrows) {
+#pragma unroll
+          for (int t = 0; t < VEC; t++)
+            ytile[i * ystride + jj * VEC + t] = acc[t];
+        }
+      }
+      __syncwarp();
+      // the tile to Y, coalesced: lanes map (row, column) by powers of two
+      const int kbv = min(KB, k - jb);
+      if (a.row_major) {
+        if (kbv <= 32) {
+          const int lc = clog2(kbv);
+          const int c = lane & ((1 << lc) - 1);
+          for (int i = lane >> lc; i < nrows; i += 32 >> lc)
+            if (c < kbv)
+              Y[((int64_t)r0 + i) * k + jb + c] = ytile[i * ystride + c];
+        } else {
+          for (int i = 0; i < nrows; i++)
+            for (int c = lane; c < kbv; c += 32)
+              Y[((int64_t)r0 + i) * k + jb + c] = ytile[i * ystride + c];
+        }
+      } else {
+        const int lr = clog2(nrows);
+        const int i = lane & ((1 << lr) - 1);
+        for (int c = lane >> lr; c < kbv; c += 32 >> lr)
+          if (i < nrows)
+            Y[((int64_t)r0 + i) + (int64_t)(jb + c) * m] = ytile[i * ystride + c];
+      }
+      __syncwarp();
+    } else {
+      // ---- one long row, staged cap nonzeros at a time into stage st ----
+      const int64_t lo0 = bm->rowptr[r0], hi0 = bm->rowptr[r0 + 1];
+      A acc[VEC];
+#pragma unroll
+      for (int t = 0; t < VEC; t++)
+        acc[t] = 0;
+      for (int64_t lo = lo0; lo < hi0; lo += a.cap) {
+        const int len = (int)min((int64_t)a.cap, hi0 - lo);
+        copy16s<int32_t>(colS, bm->colind, lo, len, lane);
+        copy16s<V>(valS, static_cast<const V *>(bm->vals), lo, len, lane);
+        cp_commit();
+        cp_wait<0>();
+        __syncwarp();
+        if (con)
+          row_sums<V, XT, VEC, A>(colS + 4 * (int)(lo & 3),
+                                  valS + (uint32_t)sizeof(V) * (int)(lo & VOFF_MASK),
+                                  slot, len, Xl, ldx, S, acc);
+        __syncwarp();
+      }
+      for (int dd = 1; dd < S; dd <<= 1) {
+#pragma unroll
+        for (int t = 0; t < VEC; t++) {
+          const A o = __shfl_down_sync(0xffffffffu, acc[t], dd * KP);
+          if ((slot & (2 * dd - 1)) == 0 && slot + dd < S)
+            acc[t] += o;
+        }
+      }
+      if (slot == 0 && con) {
+#pragma unroll
+        for (int t = 0; t < VEC; t++) {
+          const int c = c0 + t;
+          if (c < k) {
+            if (a.row_major)
+              Y[(int64_t)r0 * k + c] = acc[t];
+            else
+              Y[(int64_t)r0 + (int64_t)c * m] = acc[t];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    rec = rec_n;
+    rec_n = rec_nn;
+  }
+#undef DRB_BATCH_PAIRS
+  cp_wait<0>();
+}
+
+// dst[r*ldx + j] = X(r, j) for j < k, 0 for k <= j < ldx, from column-major
+// (src[r + j*n]) or row-major (src[r*k + j]) X.  A CTA moves a tile of
+// 2^LTR rows x 2^LCW columns through shared memory (row stride 2^LTR + 1,
+// conflict-free both ways): column-major sources are read one column at a
+// time (coalesced), and with vec the tile's rows are written as 16-byte
+// vectors.  blockIdx.x is a tile of the whole batch, mapped to its matrix by
+// binary search of the tile offsets.
+template <class T, bool COLMAJOR>
+__global__ void __launch_bounds__(256)
+    batch_pack(const PackEnt *__restrict__ ents, int count, int64_t k,
+               int64_t ldx, int lcw, int ltr, int ctiles, int vec) {
+  extern __shared__ __align__(16) unsigned char pack_smem[];
+  T *tile = reinterpret_cast<T *>(pack_smem); // [cw][tr + 1]
+  const int cw = 1 << lcw, tr = 1 << ltr, ts = tr + 1;
+  const int64_t t = blockIdx.x;
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ents[mid].tile0 <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const PackEnt e = ents[lo];
+  const int64_t lt = t - e.tile0;
+  const int64_t rb = (lt / ctiles) << ltr;
+  const int64_t cb = (lt % ctiles) << lcw;
+  const T *src = static_cast<const T *>(e.src);
+  T *dst = static_cast<T *>(e.dst);
+  const int nrow = (int)min((int64_t)tr, e.n - rb);   // rows in this tile
+  const int ncol = (int)min((int64_t)cw, ldx - cb);   // packed columns
+  const int kcol = (int)max((int64_t)0, min((int64_t)cw, k - cb)); // source
+  if (COLMAJOR) {
+    for (int j = 0; j < kcol; j++) {
+      const T *sp = src + (cb + j) * e.n + rb;
+      for (int r = threadIdx.x; r < nrow; r += blockDim.x)
+        tile[j * ts + r] = sp[r];
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < (nrow << lcw); idx += blockDim.x) {
+      const int j = idx & (cw - 1), r = idx >> lcw;
+      if (j < kcol)
+        tile[j * ts + r] = src[(rb + r) * k + cb + j];
+    }
+  }
+  for (int j = kcol; j < ncol; j++)
+    for (int r = threadIdx.x; r < nrow; r += blockDim.x)
+      tile[j * ts + r] = T(0);
+  __syncthreads();
+  constexpr int VW = 16 / (int)sizeof(T);
+  if (vec) { // ldx and cw are multiples of VW: 16-byte row pieces
+    const int lv = lcw - __ffs(VW) + 1; // log2(cw / VW)
+    for (int idx = threadIdx.x; idx < (nrow << lv); idx += blockDim.x) {
+      const int j0 = (idx & ((1 << lv) - 1)) * VW, r = idx >> lv;
+      if (j0 < ncol) {
+        union {
+          uint4 u;
+          T v[VW];
+        } w;
+#pragma unroll
+        for (int i = 0; i < VW; i++)
+          w.v[i] = tile[(j0 + i) * ts + r];
+        *reinterpret_cast<uint4 *>(dst + (rb + r) * ldx + cb + j0) = w.u;
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < (nrow << lcw); idx += blockDim.x) {
+      const int j = idx & (cw - 1), r = idx >> lcw;
+      if (j < ncol)
+        dst[(rb + r) * ldx + cb + j] = tile[j * ts + r];
+    }
+  }
+}
+
+using KernelFn = void (*)(const BArgs);
+
+template <class V, class XT> KernelFn pick_vec(int vec) {
+  if constexpr (sizeof(XT) == 2) {
+    switch (vec) {
+    case 2: return batch_spmm<V, XT, 2>;
+    case 4: return batch_spmm<V, XT, 4>;
+    case 8: return batch_spmm<V, XT, 8>;
+    }
+  } else if constexpr (sizeof(XT) == 4) {
+    switch (vec) {
+    case 1: return batch_spmm<V, XT, 1>;
+    case 2: return batch_spmm<V, XT, 2>;
+    case 4: return batch_spmm<V, XT, 4>;
+    }
+  } else {
+    switch (vec) {
+    case 1: return batch_spmm<V, XT, 1>;
+    case 2: return batch_spmm<V, XT, 2>;
+    }
+  }
+  return nullptr;
+}
+
+KernelFn pick_kernel(drb_dtype storage, bool x_f32, int vec) {
+  switch (storage) {
+  case DRB_F32:
+    return pick_vec<float, float>(vec);
+  case DRB_F64:
+    return pick_vec<double, double>(vec);
+  case DRB_BF16:
+    return x_f32 ? pick_vec<uint16_t, float>(vec)
+                 : pick_vec<uint16_t, uint16_t>(vec);
+  }
+  return nullptr;
+}
+
+template <class... Args>
+drb_status fail(drb_status st, const char *fmt, Args... args) {
+  set_error(fmt, args...);
+  return st;
+}
+
+int round16(int64_t b) { return (int)((b + 15) / 16 * 16); }
+
+} // namespace
+
+struct Batch {
+  int device = 0;
+  int count = 0;
+  drb_dtype storage = DRB_F32;
+  bool x_f32 = false;
+  int64_t k = 1;
+  drb_layout layout = DRB_COL_MAJOR;
+  bool xy_row_major = false; // X and Y are addressed row-major
+  int vbytes = 4, xbytes = 4, abytes = 4;
+  int vec = 1, ldx = 1, KP = 1, S = 32, KB = 1, nkb = 1;
+  bool pack = false;
+  int variant = -1, cap = 0, G = 1, rmax = kRmax;
+  double avg_row = 0;
+  int64_t nitems = 0;
+  int grid = 0, warps = 0;
+  BArgs args{};
+  int64_t pack_tiles = 0;
+  int pack_lcw = 0, pack_ltr = 5, pack_ctiles = 1;
+  std::vector<Csr *> mats;
+  std::vector<BMat> hmats;
+  std::vector<PackEnt> hpack;
+  DevBuf dmats, items, xpack, dpack;
+  bool bound = false;
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  KernelFn kernel = nullptr;
+  int nkernels = 0;
+  ~Batch() {
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (graph)
+      cudaGraphDestroy(graph);
+  }
+};
+
+namespace {
+
+// Cut every matrix into items of whole rows (<= cap nonzeros, <= rmax rows).
+drb_status build_items(Batch &B, int cap) {
+  std::vector<int4> items;
+  std::vector<int32_t> rp;
+  int64_t rows = 0, nnz = 0;
+  for (int b = 0; b < B.count; b++) {
+    const Csr &A = *B.mats[b];
+    if (A.m == 0)
+      continue;
+    rp.resize(A.m + 1);
+    DRB_CUDA_TRY(cudaMemcpy(rp.data(), A.rowptr.p, sizeof(int32_t) * (A.m + 1),
+                            cudaMemcpyDeviceToHost));
+    rows += A.m;
+    nnz += rp[A.m];
+    int64_t r = 0;
+    while (r < A.m) {
+      const int32_t lo = rp[r];
+      if (rp[r + 1] - lo > cap) {
+        items.push_back(make_int4(b, (int)r, 0, lo));
+        r++;
+        continue;
+      }
+      int64_t r1 = r + 1;
+      while (r1 < A.m && r1 - r < B.rmax && rp[r1 + 1] - lo <= cap)
+        r1++;
+      items.push_back(
+          make_int4(b, (int)r, (int)(r1 - r) | ((rp[r1] - lo) << 8), lo));
+      r = r1;
+    }
+  }
+  B.cap = cap;
+  B.avg_row = rows ? (double)nnz / rows : 0;
+  B.nitems = (int64_t)items.size();
+  DRB_TRY(B.items.ensure(std::max<size_t>(1, items.size()) * sizeof(int4)));
+  if (!items.empty())
+    DRB_CUDA_TRY(cudaMemcpy(B.items.p, items.data(),
+                            items.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice));
+  return DRB_OK;
+}
+
+// Shared-memory layout, warps per CTA and grid for the current items and G
+// slots per row; fills B.args.
+drb_status configure(Batch &B, int G) {
+  B.G = G;
+  BArgs &a = B.args;
+  const int cap = B.cap;
+  a.cap = cap;
+  a.rmax = B.rmax;
+  // two stages (unit t and t+1), each a slice copied from the 16-byte
+  // boundary below its start, and the output tile
+  a.cols_off = 0;
+  a.cols_stage = round16((int64_t)(cap + 8) * 4);
+  a.vals_off = 2 * a.cols_stage;
+  a.vals_stage = round16((int64_t)(cap + 16) * B.vbytes);
+  a.rs_off = a.vals_off + 2 * a.vals_stage;
+  a.rs_stage = round16((int64_t)(B.rmax + 8) * 4);
+  a.y_off = a.rs_off + 2 * a.rs_stage;
+  a.warp_bytes = round16(a.y_off + (int64_t)B.rmax * (B.KB + 1) * B.abytes);
+  int optin = 0, sms = 0;
+  DRB_CUDA_TRY(cudaDeviceGetAttribute(
+      &optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B.device));
+  DRB_CUDA_TRY(
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.device));
+  const int w = std::min(kWarps, (optin - 1024) / a.warp_bytes);
+  if (w < 1)
+    return fail(DRB_ERR_UNSUPPORTED,
+                "batch: one warp needs %d bytes of shared memory",
+                a.warp_bytes);
+  B.warps = w;
+  const int smem = w * a.warp_bytes;
+  DRB_CUDA_TRY(cudaFuncSetAttribute(
+      B.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  DRB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, B.kernel,
+                                                             w * 32, smem));
+  if (per_sm < 1)
+    return fail(DRB_ERR_UNSUPPORTED, "batch kernel does not fit an SM");
+  const int64_t units = B.nitems * B.nkb;
+  const int64_t want = (units + w - 1) / w;
+  B.grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>((int64_t)per_sm * sms, want));
+  a.nunits = units;
+  a.nkb = B.nkb;
+  a.k = (int)B.k;
+  a.ldx = B.ldx;
+  a.KP = B.KP;
+  a.S = B.S;
+  a.KB = B.KB;
+  a.G = G;
+  a.row_major = B.xy_row_major;
+  a.mats = B.dmats.as<BMat>();
+  a.items = B.items.as<int4>();
+  return DRB_OK;
+}
+
+int encode_variant(int cap_idx, int G) { return (cap_idx << 4) | G; }
+
+drb_status set_variant(Batch &B, int variant) {
+  const int ci = variant >> 4, G = variant & 15;
+  // xor trees over slots need a power-of-two slot width unless G == 1
+  if (ci < 0 || ci >= kNumCaps || G < 1 || G > B.S || (G & (G - 1)) ||
+      (G > 1 && (B.KP & (B.KP - 1))))
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: batch variant %d",
+                variant);
+  if (B.cap != kCaps[ci])
+    DRB_TRY(build_items(B, kCaps[ci]));
+  DRB_TRY(configure(B, G));
+  B.variant = variant;
+  return DRB_OK;
+}
+
+// Pack (when needed) and the SpMM kernel: the sequence the graph holds.
+drb_status enqueue(Batch &B, cudaStream_t s, bool count) {
+  int n = 0;
+  if (B.pack && B.pack_tiles > 0) {
+    const int64_t k = B.k, ldx = B.ldx;
+    const PackEnt *ents = B.dpack.as<PackEnt>();
+    const bool cm = B.layout == DRB_COL_MAJOR;
+    const unsigned grid = (unsigned)B.pack_tiles;
+    const size_t sm = ((size_t)1 << B.pack_lcw) * ((1 << B.pack_ltr) + 1) *
+                      B.xbytes;
+    const int cw = B.pack_lcw, tr = B.pack_ltr, ct = B.pack_ctiles;
+    const int vw = 16 / B.xbytes; // elements per 16-byte row piece
+    const int vec = (B.ldx % vw == 0 && (1 << B.pack_lcw) % vw == 0) ? 1 : 0;
+    if (B.xbytes == 4) {
+      if (cm)
+        batch_pack<uint32_t, true><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
+      else
+        batch_pack<uint32_t, false><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
+    } else if (B.xbytes == 2) {
+      if (cm)
+        batch_pack<uint16_t, true><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
+      else
+        batch_pack<uint16_t, false><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
+    } else {
+      if (cm)
+        batch_pack<uint64_t, true><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
+      else
+        batch_pack<uint64_t, false><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
+    }
+    DRB_CUDA_TRY(cudaGetLastError());
+    n++;
+  }
+  if (B.args.nunits > 0) {
+    B.kernel<<<B.grid, B.warps * 32, (size_t)B.warps * B.args.warp_bytes, s>>>(
+        B.args);
+    DRB_CUDA_TRY(cudaGetLastError());
+    n++;
+  }
+  B.nkernels = n;
+  if (count)
+    note_launch(n);
+  return DRB_OK;
+}
+
+drb_status capture(Batch &B) {
+  if (B.exec) {
+    cudaGraphExecDestroy(B.exec);
+    B.exec = nullptr;
+  }
+  if (B.graph) {
+    cudaGraphDestroy(B.graph);
+    B.graph = nullptr;
+  }
+  cudaStream_t cs;
+  DRB_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  drb_status st = DRB_OK;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = enqueue(B, cs, false);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(cs, &g);
+    if (e == cudaSuccess && st == DRB_OK) {
+      B.graph = g;
+      e = cudaGraphInstantiate(&B.exec, g, 0);
+    } else if (g) {
+      cudaGraphDestroy(g);
+    }
+  }
+  cudaStreamDestroy(cs);
+  if (st != DRB_OK)
+    return st;
+  DRB_CUDA_TRY(e);
+  return DRB_OK;
+}
+
+drb_status launch(Batch &B, cudaStream_t s) {
+  if (!B.bound)
+    return fail(DRB_ERR_INVALID_ARG,
+                "invalid argument: batch has no x/y bound (drb_batch_bind)");
+  if (B.use_graph && B.exec) {
+    DRB_CUDA_TRY(cudaGraphLaunch(B.exec, s));
+    note_launch(B.nkernels);
+    return DRB_OK;
+  }
+  return enqueue(B, s, true);
+}
+
+drb_status make_batch(Batch &B, int32_t count, const drb_csr_t *handles,
+                      int64_t k, drb_layout layout, uint32_t flags) {
+  if (count < 1)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: count < 1");
+  if (!handles)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: handles is NULL");
+  if (k < 1 || k > (1 << 20))
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: k out of range");
+  if (layout != DRB_COL_MAJOR && layout != DRB_ROW_MAJOR)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: layout");
+  if (flags & ~DRB_FLAG_BF16_X_F32)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: flags");
+  B.count = count;
+  B.k = k;
+  B.layout = layout;
+  for (int i = 0; i < count; i++) {
+    Csr *A = handles[i];
+    if (!A)
+      return fail(DRB_ERR_INVALID_ARG, "invalid argument: handles[%d] is NULL",
+                  i);
+    if (i == 0) {
+      B.device = A->device;
+      B.storage = A->storage;
+    } else if (A->device != B.device || A->storage != B.storage) {
+      return fail(DRB_ERR_INVALID_ARG,
+                  "invalid argument: handles[%d] differs in device or storage "
+                  "type from handles[0]",
+                  i);
+    }
+    if (A->cbytes != 4 || A->rbytes != 4)
+      return fail(DRB_ERR_UNSUPPORTED,
+                  "batch needs 32-bit column indices and rowptr (handles[%d])",
+                  i);
+    if (A->m >= INT32_MAX)
+      return fail(DRB_ERR_UNSUPPORTED, "batch needs m < 2^31 (handles[%d])",
+                  i);
+    B.mats.push_back(A);
+  }
+  if ((flags & DRB_FLAG_BF16_X_F32) && B.storage != DRB_BF16)
+    return fail(DRB_ERR_INVALID_ARG,
+                "invalid argument: BF16_X_F32 needs BF16 storage");
+  B.x_f32 = (flags & DRB_FLAG_BF16_X_F32) != 0;
+  B.vbytes = dtype_bytes(B.storage);
+  B.xbytes = B.storage == DRB_BF16 ? (B.x_f32 ? 4 : 2) : B.vbytes;
+  B.abytes = B.storage == DRB_F64 ? 8 : 4;
+  // With one right-hand side both layouts are the same vector.
+  B.xy_row_major = layout == DRB_ROW_MAJOR || k == 1;
+  const int vmax = 16 / B.xbytes, vmin = B.xbytes == 2 ? 2 : 1;
+  // Row-major X is gathered in place when k splits into VEC-wide slices;
+  // otherwise (and always for column-major X with k > 1) it is packed with
+  // row stride ldx = k rounded up to VEC.
+  int vdirect = 0;
+  if (B.xy_row_major)
+    for (int v = vmax; v >= vmin; v >>= 1)
+      if (k % v == 0) {
+        vdirect = v;
+        break;
+      }
+  if (vdirect) {
+    B.pack = false;
+    B.vec = vdirect;
+    B.ldx = (int)k;
+  } else {
+    B.pack = true;
+    int v = vmin;
+    while (v < vmax && v < k)
+      v <<= 1;
+    B.vec = v;
+    B.ldx = (int)((k + v - 1) / v * v);
+  }
+  B.KP = std::min(32, B.ldx / B.vec);
+  B.S = 32 / B.KP;
+  B.KB = B.KP * B.vec;
+  B.nkb = (B.ldx + B.KB - 1) / B.KB;
+  B.rmax = std::min(kRmax, std::max(1, kYBudget / ((B.KB + 1) * B.abytes)));
+  B.kernel = pick_kernel(B.storage, B.x_f32, B.vec);
+  if (!B.kernel)
+    return fail(DRB_ERR_UNSUPPORTED,
+                "no batch kernel for this type and vector width");
+  DRB_TRY(B.dmats.alloc(sizeof(BMat) * count));
+  B.hmats.resize(count);
+  // pack tiles: 2^lcw columns x 2^ltr rows, about 32 KB of shared memory
+  B.pack_lcw = 0;
+  while ((1 << B.pack_lcw) < std::min(B.ldx, 32))
+    B.pack_lcw++;
+  B.pack_ltr = 5;
+  while ((2 << B.pack_ltr) * ((1 << B.pack_lcw) + 1) * B.xbytes <= 34816 &&
+         B.pack_ltr < 12)
+    B.pack_ltr++;
+  B.pack_ctiles = (B.ldx + (1 << B.pack_lcw) - 1) >> B.pack_lcw;
+  int64_t tiles = 0, xpack_elems = 0;
+  for (int i = 0; i < count; i++) {
+    const Csr &A = *B.mats[i];
+    BMat &bm = B.hmats[i];
+    bm.rowptr = static_cast<const int32_t *>(A.rowptr.p);
+    bm.colind = static_cast<const int32_t *>(A.colind.p);
+    bm.vals = A.vals.p;
+    bm.x = nullptr;
+    bm.y = nullptr;
+    bm.m = A.m;
+    bm.n = A.n;
+    bm.pad = 0;
+    if (B.pack) {
+      PackEnt pe;
+      pe.src = nullptr;
+      pe.dst = nullptr;
+      pe.n = A.n;
+      pe.tile0 = tiles;
+      B.hpack.push_back(pe);
+      tiles += ((A.n + (1 << B.pack_ltr) - 1) >> B.pack_ltr) * B.pack_ctiles;
+      xpack_elems += (A.n * B.ldx + 15) / 16 * 16; // 16-element aligned
+    }
+  }
+  if (tiles > INT32_MAX)
+    return fail(DRB_ERR_UNSUPPORTED, "batch X too large to pack");
+  B.pack_tiles = tiles;
+  if (B.pack) {
+    DRB_TRY(B.xpack.alloc((size_t)std::max<int64_t>(1, xpack_elems) *
+                          B.xbytes));
+    DRB_TRY(B.dpack.alloc(sizeof(PackEnt) * count));
+    int64_t off = 0;
+    for (int i = 0; i < count; i++) {
+      B.hpack[i].dst =
+          static_cast<unsigned char *>(B.xpack.p) + off * B.xbytes;
+      B.hmats[i].x = B.hpack[i].dst;
+      off += (B.mats[i]->n * B.ldx + 15) / 16 * 16;
+    }
+  }
+  // default variant: staging capacity 128, G near the mean row length / 8
+  DRB_TRY(build_items(B, kCaps[1]));
+  int G = 1;
+  while ((B.KP & (B.KP - 1)) == 0 && G * 2 <= B.S && G * 2 * 8 <= B.avg_row)
+    G *= 2;
+  return set_variant(B, encode_variant(1, G));
+}
+
+drb_status bind(Batch &B, const void *const *x, void *const *y,
+                cudaStream_t s) {
+  if (!x || !y)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: x or y is NULL");
+  const size_t align = (size_t)B.vec * B.xbytes;
+  for (int i = 0; i < B.count; i++) {
+    const Csr &A = *B.mats[i];
+    if ((A.m > 0 && !y[i]) || (A.m > 0 && A.n > 0 && !x[i]))
+      return fail(DRB_ERR_INVALID_ARG,
+                  "invalid argument: x[%d] or y[%d] is NULL", i, i);
+    if (B.pack) {
+      B.hpack[i].src = x[i];
+    } else {
+      if (reinterpret_cast<uintptr_t>(x[i]) % align != 0)
+        return fail(DRB_ERR_INVALID_ARG,
+                    "invalid argument: row-major x[%d] must be %zu-byte "
+                    "aligned",
+                    i, align);
+      B.hmats[i].x = x[i];
+    }
+    B.hmats[i].y = y[i];
+  }
+  DRB_CUDA_TRY(cudaMemcpyAsync(B.dmats.p, B.hmats.data(),
+                               sizeof(BMat) * B.count, cudaMemcpyHostToDevice,
+                               s));
+  if (B.pack)
+    DRB_CUDA_TRY(cudaMemcpyAsync(B.dpack.p, B.hpack.data(),
+                                 sizeof(PackEnt) * B.count,
+                                 cudaMemcpyHostToDevice, s));
+  B.bound = true;
+  return DRB_OK;
+}
+
+drb_status autotune(Batch &B, cudaStream_t s, int *chosen) {
+  if (!B.bound)
+    return fail(DRB_ERR_INVALID_ARG,
+                "invalid argument: autotune needs x/y bound (drb_batch_bind)");
+  cudaEvent_t e0, e1;
+  DRB_CUDA_TRY(cudaEventCreate(&e0));
+  DRB_CUDA_TRY(cudaEventCreate(&e1));
+  float best = 0;
+  int bestv = B.variant;
+  bool first = true;
+  drb_status st = DRB_OK;
+  for (int ci = 0; ci < kNumCaps && st == DRB_OK; ci++) {
+    const int gmax = (B.KP & (B.KP - 1)) ? 1 : std::min(B.S, 8);
+    for (int G = 1; G <= gmax && st == DRB_OK; G *= 2) {
+      st = set_variant(B, encode_variant(ci, G));
+      if (st == DRB_ERR_UNSUPPORTED) { // too much shared memory for this k
+        clear_error();
+        st = DRB_OK;
+        continue;
+      }
+      if (st == DRB_OK)
+        st = enqueue(B, s, true); // warm-up
+      if (st != DRB_OK)
+        break;
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < 3 && st == DRB_OK; r++)
+        st = enqueue(B, s, true);
+      cudaEventRecord(e1, s);
+      if (st != DRB_OK)
+        break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        st = fail(DRB_ERR_CUDA, "batch autotune: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+        break;
+      }
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (first || ms < best) {
+        best = ms;
+        bestv = B.variant;
+        first = false;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  DRB_TRY(st);
+  DRB_TRY(set_variant(B, bestv));
+  if (B.use_graph)
+    DRB_TRY(capture(B));
+  if (chosen)
+    *chosen = bestv;
+  return DRB_OK;
+}
+
+} // namespace
+} // namespace drb
+
+using namespace drb;
+
+struct drb_batch_plan : public Batch {};
+
+extern "C" {
+
+drb_status drb_batch_create(drb_batch_t *out, int32_t count,
+                            const drb_csr_t *handles, int64_t k,
+                            drb_layout layout, uint32_t flags, void *stream) {
+  clear_error();
+  if (!out)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: out is NULL");
+  *out = nullptr;
+  if (count < 1 || !handles || !handles[0]) {
+    Batch probe;
+    return make_batch(probe, count, handles, k, layout, flags);
+  }
+  DeviceGuard g(handles[0]->device);
+  auto P = std::make_unique<drb_batch_plan>();
+  DRB_TRY(make_batch(*P, count, handles, k, layout, flags));
+  DRB_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  DRB_TRY(capture(*P));
+  *out = P.release();
+  return DRB_OK;
+}
+
+drb_status drb_batch_bind(drb_batch_t B, const void *const *x, void *const *y,
+                          void *stream) {
+  clear_error();
+  if (!B)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: batch is NULL");
+  DeviceGuard g(B->device);
+  return bind(*B, x, y, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_batch_gemv(drb_batch_t B, void *stream) {
+  clear_error();
+  if (!B)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: batch is NULL");
+  DeviceGuard g(B->device);
+  return launch(*B, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_batch_variant(drb_batch_t B, int *variant) {
+  clear_error();
+  if (!B || !variant)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: NULL argument");
+  *variant = B->variant;
+  return DRB_OK;
+}
+
+drb_status drb_batch_set_variant(drb_batch_t B, int variant) {
+  clear_error();
+  if (!B)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: batch is NULL");
+  DeviceGuard g(B->device);
+  DRB_TRY(set_variant(*B, variant));
+  if (B->use_graph)
+    DRB_TRY(capture(*B));
+  return DRB_OK;
+}
+
+drb_status drb_batch_autotune(drb_batch_t B, int *variant, void *stream) {
+  clear_error();
+  if (!B)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: batch is NULL");
+  DeviceGuard g(B->device);
+  return autotune(*B, static_cast<cudaStream_t>(stream), variant);
+}
+
+drb_status drb_batch_destroy(drb_batch_t B) {
+  clear_error();
+  if (!B)
+    return DRB_OK;
+  DeviceGuard g(B->device);
+  delete B;
+  return DRB_OK;
+}
+
+drb_status drb_batched_gemv(int32_t count, const drb_csr_t *handles,
+                            const void *const *x, void *const *y, int64_t k,
+                            drb_layout layout, uint32_t flags, void *stream) {
+  clear_error();
+  Batch probe;
+  if (count < 1 || !handles || !handles[0])
+    return make_batch(probe, count, handles, k, layout, flags);
+  DeviceGuard g(handles[0]->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  probe.use_graph = false;
+  DRB_TRY(make_batch(probe, count, handles, k, layout, flags));
+  DRB_TRY(bind(probe, x, y, s));
+  DRB_TRY(launch(probe, s));
+  DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  return DRB_OK;
+}
+
+} // extern "C"

@@ -23,20 +23,6 @@ std::atomic<uint64_t> g_launch_count{0};
 namespace {
 thread_local std::string t_error;
 
-struct DeviceGuard {
-  int prev = -1;
-  bool switched = false;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) {
-      switched = cudaSetDevice(dev) == cudaSuccess;
-    }
-  }
-  ~DeviceGuard() {
-    if (switched)
-      cudaSetDevice(prev);
-  }
-};
-
 drb_status invalid(const char *msg) {
   set_error("invalid argument: %s", msg);
   return DRB_ERR_INVALID_ARG;
@@ -245,8 +231,6 @@ Csr::~Csr() = default;
 } // namespace drb
 
 using namespace drb;
-
-struct drb_csr_matrix : public Csr {};
 
 extern "C" {
 

@@ -47,6 +47,21 @@ void clear_error();
 extern std::atomic<uint64_t> g_launch_count;
 inline void note_launch(uint64_t n = 1) { g_launch_count.fetch_add(n); }
 
+// Makes `dev` current for the scope of an entry point, restoring the
+// caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != dev)
+      switched = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (switched)
+      cudaSetDevice(prev);
+  }
+};
+
 // ---- device buffers ----------------------------------------------------------
 struct DevBuf {
   void *p = nullptr;
@@ -192,6 +207,9 @@ inline int dtype_bytes(drb_dtype t) {
 }
 
 } // namespace drb
+
+// The opaque handle type of drb.h is the library's Csr.
+struct drb_csr_matrix : public drb::Csr {};
 
 // ---- PTX helpers ---------------------------------------------------------------
 namespace drb::ptx {

@@ -83,6 +83,16 @@ DRB_SYMBOLS = [
     ("drb_csr_residual_norm2", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("drb_csr_gemv_backward", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("drb_csr_update_values", _st, [_vp, _vp, _vp]),
+    ("drb_batch_create", _st, [C.POINTER(_vp), _i32, C.POINTER(_vp), _i64, _i32,
+                               _u32, _vp]),
+    ("drb_batch_bind", _st, [_vp, C.POINTER(_vp), C.POINTER(_vp), _vp]),
+    ("drb_batch_gemv", _st, [_vp, _vp]),
+    ("drb_batch_variant", _st, [_vp, C.POINTER(_i32)]),
+    ("drb_batch_set_variant", _st, [_vp, _i32]),
+    ("drb_batch_autotune", _st, [_vp, C.POINTER(_i32), _vp]),
+    ("drb_batch_destroy", _st, [_vp]),
+    ("drb_batched_gemv", _st, [_i32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                               _i64, _i32, _u32, _vp]),
     ("drb_dense_gemv", _st, [_i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _i32, _vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_dot_noalloc", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),

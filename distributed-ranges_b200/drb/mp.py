@@ -26,7 +26,7 @@ __all__ = [
     "csr_matrix_view", "distribution", "csr_row_distribution",
     "csr_eq_distribution", "distributed_sparse_matrix", "broadcasted_vector",
     "broadcasted_slim_matrix", "gemv", "gemv_backward", "dense_gemv", "dot",
-    "residual_norm2", "default_comm", "init", "finalize",
+    "residual_norm2", "default_comm", "init", "finalize", "batch", "batched_gemv",
 ]
 
 _TORCH_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
@@ -456,6 +456,80 @@ def gemv(*args, stream=None) -> None:
     if x.dtype != a.x_dtype:
         x = x.to(a.x_dtype)
     a.local_gemv_and_collect(root, res, x, width, stream=stream)
+
+
+def _ptr_array(ts) -> C.Array:
+    return (C.c_void_p * len(ts))(*[_ptr(t).value for t in ts])
+
+
+class batch:
+    """Y_i = A_i X_i for many matrices in one persistent launch replayed from
+    a CUDA graph (drb_batch_*).  X_i is n_i x k and Y_i is m_i x k in
+    ``layout`` (column-major by default, the broadcasted_slim_matrix layout).
+    The matrices must outlive the batch."""
+
+    def __init__(self, mats: Sequence[distributed_sparse_matrix], k: int,
+                 layout: int = capi.DRB_COL_MAJOR, stream=None):
+        self._b = C.c_void_p(0)
+        self._mats = list(mats)
+        self.k = int(k)
+        self.layout = layout
+        hs = (C.c_void_p * len(self._mats))(*[m.handle.value for m in self._mats])
+        flags = 0
+        if self._mats and self._mats[0].x_dtype == torch.float32 and \
+                self._mats[0].storage_bytes()[0] == 2:
+            flags |= capi.DRB_FLAG_BF16_X_F32
+        h = C.c_void_p(0)
+        check(capi.lib.drb_batch_create(C.byref(h), len(self._mats), hs, self.k,
+                                        layout, flags, _stream(stream)))
+        self._b = h
+        self._bound = None
+
+    def bind(self, xs: Sequence[torch.Tensor], ys: Sequence[torch.Tensor],
+             stream=None) -> None:
+        if len(xs) != len(self._mats) or len(ys) != len(self._mats):
+            raise ValueError("one x and one y per matrix")
+        self._bound = (list(xs), list(ys))  # keep the tensors alive
+        check(capi.lib.drb_batch_bind(self._b, _ptr_array(xs), _ptr_array(ys),
+                                      _stream(stream)))
+
+    def gemv(self, stream=None) -> None:
+        check(capi.lib.drb_batch_gemv(self._b, _stream(stream)))
+
+    def variant(self) -> int:
+        v = C.c_int(0)
+        check(capi.lib.drb_batch_variant(self._b, C.byref(v)))
+        return v.value
+
+    def set_variant(self, variant: int) -> None:
+        check(capi.lib.drb_batch_set_variant(self._b, int(variant)))
+
+    def autotune(self, stream=None) -> int:
+        v = C.c_int(0)
+        check(capi.lib.drb_batch_autotune(self._b, C.byref(v), _stream(stream)))
+        return v.value
+
+    def destroy(self) -> None:
+        if self._b and self._b.value:
+            capi.lib.drb_batch_destroy(self._b)
+            self._b = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def batched_gemv(mats: Sequence[distributed_sparse_matrix], xs, ys, k: int,
+                 layout: int = capi.DRB_COL_MAJOR, stream=None) -> None:
+    """One-shot batch: Y_i = A_i X_i for all i (synchronises the stream)."""
+    hs = (C.c_void_p * len(mats))(*[m.handle.value for m in mats])
+    flags = 0
+    if mats and mats[0].x_dtype == torch.float32 and mats[0].storage_bytes()[0] == 2:
+        flags |= capi.DRB_FLAG_BF16_X_F32
+    check(capi.lib.drb_batched_gemv(len(mats), hs, _ptr_array(xs), _ptr_array(ys),
+                                    int(k), layout, flags, _stream(stream)))
 
 
 def gemv_backward(a: distributed_sparse_matrix, ybar: torch.Tensor,

@@ -27,7 +27,7 @@
  *
  * Entry points with no reference counterpart (new API shaped after gemv):
  *   drb_dense_gemv, drb_dot, drb_csr_residual_norm2, drb_csr_gemv_backward,
- *   drb_csr_update_values, drb_batch_*.
+ *   drb_csr_update_values, drb_batch_*, drb_batched_gemv.
  *
  * Layouts.  Multi-RHS blocks follow broadcasted_slim_matrix: column-major,
  * x[c + j*n], y[r + j*m] (gemv.hpp:29-39, csr_row_distribution.hpp:129-130).
@@ -169,6 +169,55 @@ drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
  * refresh the CSC copy used by gemv_backward. */
 drb_status drb_csr_update_values(drb_csr_t A, const void *values,
                                  void *stream);
+
+/* ---- batched execution ---------------------------------------------------
+ * Y_i = A_i X_i for many handles in ONE persistent kernel launch, replayed
+ * from a CUDA graph.  The reference multiplies one matrix per gemv call
+ * (include/dr/mp/algorithms/matrix/gemv.hpp:29-39 with a
+ * broadcasted_slim_matrix of k columns); a batch is that call for `count`
+ * matrices at once.  X_i is n_i x k and Y_i is m_i x k, both in `layout`
+ * (DRB_COL_MAJOR is the reference's slim-matrix layout, x[c + j*n]).
+ * Element types as drb_csr_gemv: the storage type, or for BF16 storage bf16
+ * X (f32 with DRB_FLAG_BF16_X_F32) and f32 Y; BF16 sums are plain f32.
+ * Handles must share the device and the storage type, have 32-bit rowptr and
+ * column indices (nnz < 2^31 each), and must outlive the batch. */
+typedef struct drb_batch_plan *drb_batch_t;
+
+/* Build the batch's work list and capture its graph.  flags: 0 or
+ * DRB_FLAG_BF16_X_F32.  The call synchronises `stream`. */
+drb_status drb_batch_create(drb_batch_t *out, int32_t count,
+                            const drb_csr_t *handles, int64_t k,
+                            drb_layout layout, uint32_t flags, void *stream);
+
+/* Bind the device pointers x[i], y[i] (arrays of `count` pointers, read
+ * during the call).  The pointer table is updated in stream order, so later
+ * launches on `stream` see it; rebinding needs no new graph.  Row-major X
+ * must be aligned to the kernel's vector width (16 bytes always suffices). */
+drb_status drb_batch_bind(drb_batch_t B, const void *const *x, void *const *y,
+                          void *stream);
+
+/* Launch the captured graph on `stream` (asynchronous).  A batch is not
+ * reentrant: do not overlap two launches of the same batch. */
+drb_status drb_batch_gemv(drb_batch_t B, void *stream);
+
+/* Kernel variant: (c << 4) | G, with staging capacity 128 << c nonzeros per
+ * work unit (c = 0, 1, 2) and G slots summing one row (1, 2, 4, 8).  The
+ * default is c = 1 with G from the mean row length.  Results depend on G
+ * only (the order of each row's sum), not on c, for rows of at most 128
+ * nonzeros.  drb_batch_set_variant re-captures the graph;
+ * drb_batch_autotune times every variant with the bound x and y (which it
+ * overwrites with the product), keeps the fastest, re-captures the graph and
+ * synchronises `stream`. */
+drb_status drb_batch_variant(drb_batch_t B, int *variant);
+drb_status drb_batch_set_variant(drb_batch_t B, int variant);
+drb_status drb_batch_autotune(drb_batch_t B, int *variant, void *stream);
+
+drb_status drb_batch_destroy(drb_batch_t B);
+
+/* One-shot form: create, bind, launch (no graph), synchronise, destroy. */
+drb_status drb_batched_gemv(int32_t count, const drb_csr_t *handles,
+                            const void *const *x, void *const *y, int64_t k,
+                            drb_layout layout, uint32_t flags, void *stream);
 
 /* ---- dense and reductions ------------------------------------------------ */
 

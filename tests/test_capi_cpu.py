@@ -87,6 +87,27 @@ def test_gemv_rejects_null_handle():
         capi.DRB_ERR_INVALID_ARG
 
 
+def test_batch_rejects_bad_arguments_without_gpu():
+    lib = capi.lib
+    out = C.c_void_p()
+    hs = (C.c_void_p * 2)(None, None)
+    assert lib.drb_batch_create(None, 1, hs, 16, 0, 0, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_batch_create(C.byref(out), 0, hs, 16, 0, 0, None) == \
+        capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_batch_create(C.byref(out), 2, None, 16, 0, 0, None) == \
+        capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_batch_create(C.byref(out), 2, hs, 16, 0, 0, None) == \
+        capi.DRB_ERR_INVALID_ARG
+    assert "handles" in capi.last_error()
+    assert not out.value
+    assert lib.drb_batch_gemv(None, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_batch_bind(None, None, None, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_batch_autotune(None, None, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_batch_destroy(None) == capi.DRB_OK
+    assert lib.drb_batched_gemv(0, hs, None, None, 16, 0, 0, None) == \
+        capi.DRB_ERR_INVALID_ARG
+
+
 def test_zipf_alpha_solver():
     a = drb.gen.zipf_alpha_for_mean(1, 16384, 20.0)
     assert abs(a - 1.7613) < 1e-3
