@@ -14,7 +14,9 @@ the 126 MB L2, so no L2 flush is needed between steps.
   e2e    the same metric through drb_csr_gemv_host: x copied from pinned host
          memory, SpMV, y copied back, every step
   extra  FP64 SpMV, the adjoint (gemv_backward), the fused residual, dense
-         32768^2 gemv, each with its own GB/s
+         32768^2 gemv, each with its own GB/s; the batched SpMM of 512 CSR
+         matrices with 16 right-hand sides (FP32 and BF16, one CUDA-graph
+         launch per step)
 
 --impl reference times the reference's CPU algorithm for the same workload
 (the csr_row_distribution CPU loop restated in oracle/, one thread per host
@@ -273,6 +275,8 @@ def run_ours(args):
     extra = {}
     if not args.no_extra:
         extra = extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes_, kern_ms, stream)
+        if not args.no_batch:
+            extra["batched"] = batch_extras(args, stream)
 
     line = None
     if rank == 0:
@@ -379,6 +383,81 @@ def extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes32, fwd_ms, stream):
     return out
 
 
+BATCH_COUNT = 512
+BATCH_K = 16
+ROW_GATHER_CEILING = {64: 183e9, 32: 234e9}  # rows/s, register gathers of 64/32-B rows
+
+
+def batch_extras(args, stream):
+    """Batched SpMM: 512 square CSR matrices (rows ~ U[1024, 200000], nnz/row
+    ~ U[8, 64], uniform distinct columns, values and X ~ U(-1, 1)), k = 16
+    right-hand sides in the reference's column-major layout, one graph launch
+    per step; FP32 and BF16 storage (bf16 X, f32 Y)."""
+    import torch
+    import drb
+    from drb import mp
+    peak, _ = hbm_peak()
+    steps = max(3, min(args.steps, 10))
+    k = BATCH_K
+    rng = np.random.default_rng(SEED + 5)
+    ms_rows = rng.integers(1024, 200001, size=BATCH_COUNT)
+    g = torch.Generator(device="cuda").manual_seed(SEED + 6)
+    m32, mbf, xs, xbf, ys32, ysbf = [], [], [], [], [], []
+    nnz = 0
+    t0 = time.time()
+    for i, m in enumerate(ms_rows):
+        m = int(m)
+        rp, ci, v = drb.gen.uniform_rows_csr(m, m, lo=8, hi=64, seed=SEED + 1000 + i)
+        nnz += int(rp[-1])
+        view = mp.csr_matrix_view(v, rp, ci, (m, m))
+        m32.append(mp.distributed_sparse_matrix(view, 0, distr=mp.csr_row_distribution))
+        mbf.append(mp.distributed_sparse_matrix(view, 0, distr=mp.csr_row_distribution,
+                                                storage=torch.bfloat16))
+        x = torch.empty(m * k, device="cuda").uniform_(-1, 1, generator=g)
+        xs.append(x)
+        xbf.append(x.to(torch.bfloat16))
+        ys32.append(torch.empty(m * k, device="cuda"))
+        ysbf.append(torch.empty(m * k, device="cuda"))
+    gen_s = time.time() - t0
+    rows = int(ms_rows.sum())
+    out = {"config": {"matrices": BATCH_COUNT, "rows": "U[1024,200000]",
+                      "nnz_per_row": "U[8,64]", "k": k, "layout": "column-major X and Y",
+                      "total_rows": rows, "total_nnz": nnz,
+                      "setup_s": round(gen_s, 1)}}
+    res = {}
+    for name, mats, xx, yy, vb, xb in (("fp32", m32, xs, ys32, 4, 4),
+                                        ("bf16", mbf, xbf, ysbf, 2, 2)):
+        b = mp.batch(mats, k, 0)
+        b.bind(xx, yy)
+        variant = b.autotune()
+        for _ in range(2):
+            b.gemv()
+        ms = statistics.mean(timed_launches(b.gemv, steps, stream))
+        byts = nnz * (4 + vb) + (rows + BATCH_COUNT) * 4 + rows * k * (xb + 4)
+        gbps = byts / (ms * 1e-3) / 1e9
+        rate = nnz / (ms * 1e-3)
+        res[name] = ms
+        out["batch_" + name] = {
+            "ms": round(ms, 3), "GBps": round(gbps, 1), "frac": round(gbps / peak, 4),
+            "gflops": round(2 * nnz * k / (ms * 1e-3) / 1e9, 1),
+            "gathers_per_s": round(rate / 1e9, 2),
+            "gather_ceiling_frac": round(rate / ROW_GATHER_CEILING[k * xb], 4),
+            "variant": "cap=%d G=%d" % (128 << (variant >> 4), variant & 15),
+            "alg_bytes": byts, "launches_per_step": 2}
+        b.destroy()
+    torch.cuda.synchronize()
+    # bf16 against fp32 on the same inputs: norm-wise relative difference
+    num = sum(float(torch.sum((a.double() - c.double()) ** 2)) for a, c in zip(ysbf, ys32))
+    den = sum(float(torch.sum(c.double() ** 2)) for c in ys32)
+    out["bf16_vs_fp32"] = {"speedup": round(res["fp32"] / res["bf16"], 3),
+                           "normwise_rel_diff": float("%.3e" % ((num / den) ** 0.5))}
+    for a in m32 + mbf:
+        a.destroy()
+    del xs, xbf, ys32, ysbf
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,6 +466,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 512-matrix batched SpMM extra")
     ap.add_argument("--rows", type=int, default=M,
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
