@@ -94,6 +94,13 @@ DRB_SYMBOLS = [
     ("drb_batched_gemv", _st, [_i32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
                                _i64, _i32, _u32, _vp]),
     ("drb_dense_gemv", _st, [_i64, _i64, _vp, _i64, _vp, _vp, _i64, _i32, _i32, _vp]),
+    ("drb_dense_batch_create", _st, [C.POINTER(_vp), _i32, C.POINTER(_i64), C.POINTER(_i64),
+                                     C.POINTER(_vp), C.POINTER(_i64), C.POINTER(_vp),
+                                     C.POINTER(_vp), _i64, _i32, _i32, _vp]),
+    ("drb_dense_batch_gemv", _st, [_vp, _vp]),
+    ("drb_dense_batch_set_variant", _st, [_vp, _i32]),
+    ("drb_dense_batch_check", _st, [_vp, _vp]),
+    ("drb_dense_batch_destroy", _st, [_vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_dot_noalloc", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_malloc", _st, [C.POINTER(_vp), C.c_size_t]),

@@ -27,6 +27,7 @@ __all__ = [
     "csr_eq_distribution", "distributed_sparse_matrix", "broadcasted_vector",
     "broadcasted_slim_matrix", "gemv", "gemv_backward", "dense_gemv", "dot",
     "residual_norm2", "default_comm", "init", "finalize", "batch", "batched_gemv",
+    "dense_batch",
 ]
 
 _TORCH_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
@@ -556,6 +557,50 @@ def dense_gemv(A: torch.Tensor, x: torch.Tensor, y: torch.Tensor, k: int = 1,
     lda = A.stride(0)
     check(capi.lib.drb_dense_gemv(m, n, _ptr(A), lda, _ptr(x), _ptr(y), int(k), layout,
                                   _TORCH_DT[A.dtype], _stream(stream)))
+
+
+class dense_batch:
+    """Y_i = A_i X_i for row-major BF16 matrices on the tensor cores
+    (drb_dense_batch_*): A_i a 2-D bf16 tensor (rows may be padded: its
+    stride(0) is the leading dimension, a multiple of 8), X_i n_i x k bf16 and
+    Y_i m_i x k fp32, flat, in ``layout``.  The tensors must outlive the plan."""
+
+    def __init__(self, As: Sequence[torch.Tensor], xs: Sequence[torch.Tensor],
+                 ys: Sequence[torch.Tensor], k: int, layout: int = capi.DRB_COL_MAJOR,
+                 ns: Sequence[int] | None = None, stream=None):
+        cnt = len(As)
+        if not (len(xs) == len(ys) == cnt):
+            raise ValueError("one x and one y per matrix")
+        self._keep = (list(As), list(xs), list(ys))
+        m = (C.c_int64 * cnt)(*[a.shape[0] for a in As])
+        n = (C.c_int64 * cnt)(*(ns if ns is not None else [a.shape[1] for a in As]))
+        lda = (C.c_int64 * cnt)(*[a.stride(0) for a in As])
+        h = C.c_void_p(0)
+        self._p = C.c_void_p(0)
+        check(capi.lib.drb_dense_batch_create(C.byref(h), cnt, m, n, _ptr_array(As), lda,
+                                              _ptr_array(xs), _ptr_array(ys), int(k),
+                                              layout, capi.DRB_BF16, _stream(stream)))
+        self._p = h
+
+    def gemv(self, stream=None) -> None:
+        check(capi.lib.drb_dense_batch_gemv(self._p, _stream(stream)))
+
+    def set_variant(self, variant: int) -> None:
+        check(capi.lib.drb_dense_batch_set_variant(self._p, int(variant)))
+
+    def check(self, stream=None) -> None:
+        check(capi.lib.drb_dense_batch_check(self._p, _stream(stream)))
+
+    def destroy(self) -> None:
+        if self._p and self._p.value:
+            capi.lib.drb_dense_batch_destroy(self._p)
+            self._p = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 def dot(a: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None,

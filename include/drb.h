@@ -27,7 +27,7 @@
  *
  * Entry points with no reference counterpart (new API shaped after gemv):
  *   drb_dense_gemv, drb_dot, drb_csr_residual_norm2, drb_csr_gemv_backward,
- *   drb_csr_update_values, drb_batch_*, drb_batched_gemv.
+ *   drb_csr_update_values, drb_batch_*, drb_batched_gemv, drb_dense_batch_*.
  *
  * Layouts.  Multi-RHS blocks follow broadcasted_slim_matrix: column-major,
  * x[c + j*n], y[r + j*m] (gemv.hpp:29-39, csr_row_distribution.hpp:129-130).
@@ -226,6 +226,33 @@ drb_status drb_batched_gemv(int32_t count, const drb_csr_t *handles,
 drb_status drb_dense_gemv(int64_t m, int64_t n, const void *A, int64_t lda,
                           const void *x, void *y, int64_t k, drb_layout layout,
                           drb_dtype dtype, void *stream);
+
+/* Batched dense multi-RHS product on the tensor cores: Y_i = A_i X_i for
+ * `count` row-major BF16 matrices A_i (m[i] x n[i], leading dimension lda[i]:
+ * a multiple of 8, A_i 16-byte aligned) and BF16 X_i (n[i] x k, 1 <= k <=
+ * 256) in `layout`; Y_i (m[i] x k, `layout`) is FP32, accumulated in FP32
+ * (tcgen05.mma into tensor memory).  dtype must be DRB_BF16.  The plan binds
+ * the pointers and is launched any number of times; all matrices run in one
+ * kernel (plus one small kernel that lays every X out K-major).  No
+ * reference counterpart: it is gemv's multi-RHS form for a batch of dense
+ * matrices (the reference's dense product is local_gemm,
+ * include/dr/sp/algorithms/matrix/local_gemm.hpp:18-62). */
+typedef struct drb_dense_batch_plan *drb_dense_batch_t;
+drb_status drb_dense_batch_create(drb_dense_batch_t *out, int32_t count,
+                                  const int64_t *m, const int64_t *n,
+                                  const void *const *A, const int64_t *lda,
+                                  const void *const *x, void *const *y,
+                                  int64_t k, drb_layout layout,
+                                  drb_dtype dtype, void *stream);
+drb_status drb_dense_batch_gemv(drb_dense_batch_t P, void *stream);
+/* TMA ring variant {stages, 64-wide K boxes per stage}: 0 = {4, 1},
+ * 1 = {5, 1} (the default), 2 = {8, 1}, 3 = {2, 2}, 4 = {4, 2}.  Results do
+ * not depend on the variant. */
+drb_status drb_dense_batch_set_variant(drb_dense_batch_t P, int variant);
+/* Synchronise `stream`; DRB_ERR_TIMEOUT when a bounded in-kernel wait of an
+ * earlier launch expired (the error word is cleared). */
+drb_status drb_dense_batch_check(drb_dense_batch_t P, void *stream);
+drb_status drb_dense_batch_destroy(drb_dense_batch_t P);
 
 /* out[0] = sum_i a[i]*b[i] (a == b gives the squared norm), f64 accumulation
  * with a deterministic order; out is a device double*.  F32 or F64. */
