@@ -14,9 +14,14 @@ the 126 MB L2, so no L2 flush is needed between steps.
   e2e    the same metric through drb_csr_gemv_host: x copied from pinned host
          memory, SpMV, y copied back, every step
   extra  FP64 SpMV, the adjoint (gemv_backward), the fused residual, dense
-         32768^2 gemv, each with its own GB/s; the batched SpMM of 512 CSR
+         32768^2 gemv, each with its own GB/s; the 131072^2 16-per-row case
+         (L2-flushed and warm); L = 0.5||Ax-b||^2 forward and backward on the
+         2048^2 Laplacian and a 4M-row power-law matrix with finite-difference
+         checks; BF16 / FP32 / compensated FP32 error per row-length bin on the
+         8M-row scaled power-law matrix; the batched SpMM of 512 CSR
          matrices with 16 right-hand sides (FP32 and BF16, one CUDA-graph
-         launch per step)
+         launch per step); the tensor-core dense product of 64 BF16 squares
+         with 32 right-hand sides
 
 --impl reference times the reference's CPU algorithm for the same workload
 (the csr_row_distribution CPU loop restated in oracle/, one thread per host
@@ -275,8 +280,12 @@ def run_ours(args):
     extra = {}
     if not args.no_extra:
         extra = extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes_, kern_ms, stream)
+        extra["config1_fixed16"] = config1_extras(args, stream)
+        extra["adjoint_fd"] = adjoint_extras(args, stream)
+        extra["precision"] = precision_extras(args, stream)
         if not args.no_batch:
             extra["batched"] = batch_extras(args, stream)
+            extra["dense_batch_bf16"] = dense_batch_extras(args, stream)
 
     line = None
     if rank == 0:
@@ -458,6 +467,332 @@ def batch_extras(args, stream):
     return out
 
 
+def l2_flusher():
+    """A callable that writes 256 MB (2x the 126 MB L2) on the GPU."""
+    import torch
+    buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    return lambda: buf.fill_(1)
+
+
+def flushed_launches(fn, steps, stream, flush):
+    """Per-launch CUDA-event durations with an L2 flush before each launch
+    (the flush itself is outside the events)."""
+    import torch
+    out = []
+    for _ in range(steps):
+        flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def config1_extras(args, stream):
+    """131,072^2 CSR with exactly 16 distinct uniform columns per row (the
+    reference's own CPU-runnable case): fits in L2, so timed both with an L2
+    flush before every launch and L2-warm."""
+    import torch
+    import drb
+    from drb import mp
+    n = 131072
+    rp, ci, v = drb.gen.fixed_rows_csr(n, n, length=16, seed=SEED + 11)
+    A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (n, n)), 0,
+                                     distr=mp.csr_row_distribution, autotune=True)
+    x = torch.from_numpy(drb.gen.values(n, seed=SEED + 12)).cuda()
+    y = torch.empty(n, device="cuda")
+    nnz = int(rp[-1])
+    byts = alg_bytes(n, n, nnz, 4, 4, 4, 4, 4)
+    for _ in range(3):
+        A.gemv_device(x, y)
+    steps = max(20, args.steps)
+    cold = statistics.median(flushed_launches(lambda: A.gemv_device(x, y), steps, stream,
+                                              l2_flusher()))
+    warm = statistics.median(timed_launches(lambda: A.gemv_device(x, y), steps, stream))
+    A.destroy()
+    return {"config": {"rows": n, "nnz": nnz, "row_len": "exactly 16", "alg_bytes": byts},
+            "l2_flushed": {"ms": round(cold, 4), "GBps": round(byts / (cold * 1e-3) / 1e9, 1)},
+            "l2_warm": {"ms": round(warm, 4), "GBps": round(byts / (warm * 1e-3) / 1e9, 1)}}
+
+
+def adjoint_extras(args, stream):
+    """L = 0.5 ||A x - b||^2: forward (fused residual) and backward (xbar =
+    A^T (A x - b) on the CSC plan, abar = r_i x_j) on the 2048^2 5-point
+    Laplacian and on the power-law matrix at 4,194,304 rows, FP64 and FP32;
+    FP64 gradients checked by central differences (h = 1e-6) on 1024 seeded
+    coordinates of x and 64 of the values."""
+    import torch
+    import drb
+    from drb import mp
+    peak, _ = hbm_peak()
+    steps = max(3, min(args.steps, 10))
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(SEED + 21)
+    mats = {"laplacian2048": None, "powerlaw_4M": None}
+    rp, ci, v = drb.gen.laplacian2d_csr(2048, value_dtype=np.float64)
+    mats["laplacian2048"] = (rp.astype(np.int32), ci, v)
+    alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
+    rp, ci, v = drb.gen.powerlaw_csr(4_194_304, 4_194_304, alpha=alpha, hi=ZIPF_HI,
+                                     seed=SEED + 22, value_dtype=np.float64)
+    mats["powerlaw_4M"] = (rp, ci, v)
+    for name, (rp, ci, v) in mats.items():
+        m = len(rp) - 1
+        nnz = int(rp[-1])
+        res = {"rows": m, "nnz": nnz}
+        for dt, npdt, eb in (("fp64", np.float64, 8), ("fp32", np.float32, 4)):
+            t0 = time.time()
+            A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v.astype(npdt), rp, ci, (m, m)),
+                                             0, distr=mp.csr_row_distribution, adjoint=True)
+            setup = time.time() - t0
+            tdt = torch.float64 if dt == "fp64" else torch.float32
+            x = torch.randn(m, device="cuda", dtype=torch.float64, generator=g).to(tdt)
+            b = torch.randn(m, device="cuda", dtype=torch.float64, generator=g).to(tdt)
+            y = torch.empty(m, device="cuda", dtype=tdt)
+            xbar = torch.empty_like(x)
+            abar = torch.empty(nnz, device="cuda", dtype=tdt)
+            fwd = lambda: mp.residual_norm2(A, x, b, y)
+            bwd = lambda: mp.gemv_backward(A, r, x, xbar, abar)
+            fwd()
+            r = y - b
+            for _ in range(2):
+                bwd()
+            f_ms = statistics.mean(timed_launches(fwd, steps, stream))
+            b_ms = statistics.mean(timed_launches(bwd, steps, stream))
+            fb = alg_bytes(m, m, nnz, eb, 4, 4, eb, eb) + eb * m  # + b for the residual
+            bb = (4 * (m + 1) + 8 * nnz + eb * nnz + eb * m + eb * m) \
+                + (4 * nnz + eb * m + eb * m + eb * nnz)  # xbar pass + abar pass
+            res[dt] = {"fwd_ms": round(f_ms, 4), "bwd_ms": round(b_ms, 4),
+                       "bwd_over_fwd": round(b_ms / f_ms, 3),
+                       "fwd_GBps": round(fb / (f_ms * 1e-3) / 1e9, 1),
+                       "bwd_GBps": round(bb / (b_ms * 1e-3) / 1e9, 1),
+                       "bwd_frac": round(bb / (b_ms * 1e-3) / 1e9 / peak, 4),
+                       "setup_s_incl_csc_plan": round(setup, 2)}
+            if dt == "fp64":
+                Aabs = mp.distributed_sparse_matrix(
+                    mp.csr_matrix_view(np.abs(v), rp, ci, (m, m)), 0,
+                    distr=mp.csr_row_distribution, adjoint=True)
+                xscale = torch.empty_like(x)
+                mp.gemv_backward(Aabs, r.abs(), None, xscale, None)  # (|A|^T |r|)_i
+                Aabs.destroy()
+                res[dt]["fd"] = fd_check(A, x, b, r, xbar, abar, xscale, v, rp, m)
+                del xscale
+            A.destroy()
+            del x, b, y, xbar, abar, r
+        out[name] = res
+    torch.cuda.empty_cache()
+    return out
+
+
+def fd_check(A, x, b, r, xbar, abar, xscale, v, rp, m):
+    """Central differences of L = 0.5||Ax - b||^2 (h = 1e-6, FP64) against
+    xbar on 1024 coordinates and abar on 64 stored entries.  Only the rows
+    touched by a perturbation change, so dL is summed row-wise as
+    0.5 (y+ - y-)(y+ + y- - 2b), which avoids cancelling two large sums.
+    Errors are relative to (|A|^T |r|)_i for xbar (the sum it cancels) and
+    to |abar_p| = |r_i x_j| for abar."""
+    import torch
+    h = 1e-6
+    y1 = torch.empty_like(x)
+    y2 = torch.empty_like(x)
+
+    def dl(y_p, y_m):
+        return float(torch.sum(0.5 * (y_p - y_m) * (y_p + y_m - 2 * b)))
+    rng = np.random.default_rng(SEED + 23)
+    idx = rng.choice(m, size=1024, replace=False)
+    xe = []
+    xbh = xbar.cpu().numpy()
+    xsh = xscale.cpu().numpy()
+    xp = x.clone()
+    for i in idx:
+        i = int(i)
+        xi = float(x[i])
+        xp[i] = xi + h
+        A.gemv_device(xp, y1)
+        xp[i] = xi - h
+        A.gemv_device(xp, y2)
+        xp[i] = xi
+        fd = dl(y1, y2) / (2 * h)
+        xe.append(abs(fd - xbh[i]) / max(xsh[i], 1e-300))
+    # values: perturb one stored entry at a time through update_values
+    nnz = int(rp[-1])
+    pidx = rng.choice(nnz, size=64, replace=False)
+    ae = []
+    abh = abar.cpu().numpy()
+    vals = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+    for p in pidx:
+        p = int(p)
+        vp = float(vals[p])
+        vals[p] = vp + h
+        A.update_values(vals)
+        A.gemv_device(x, y1)
+        vals[p] = vp - h
+        A.update_values(vals)
+        A.gemv_device(x, y2)
+        vals[p] = vp
+        fd = dl(y1, y2) / (2 * h)
+        ae.append(abs(fd - abh[p]) / max(abs(abh[p]), 1e-300))
+    A.update_values(vals)
+    return {"h": h, "x_coords": len(xe), "xbar_max_rel_err": float("%.3e" % max(xe)),
+            "value_coords": len(ae), "abar_max_rel_err": float("%.3e" % max(ae))}
+
+
+PREC_ROWS = 8_388_608
+PREC_HI = 65536
+PREC_MEAN = 32.0
+
+
+def precision_extras(args, stream):
+    """BF16 storage (bf16 x, and f32 x) and FP32 (plain and compensated)
+    against this library's FP64 SpMV on the power-law matrix of 8,388,608
+    rows (Zipf on [1, 65536], mean 32), values N(0,1) * 10^U(-3,3) per row,
+    x ~ U(-1,1).  Errors are relative to sum_j |a_ij x_j| (an FP64 product
+    with |A| and |x|), max and mean per row-length bin.  Effective throughput
+    = FP32-equivalent algorithmic bytes / time."""
+    import torch
+    import drb
+    from drb import mp
+    steps = max(3, min(args.steps, 10))
+    m = PREC_ROWS
+    alpha = drb.gen.zipf_alpha_for_mean(1, PREC_HI, PREC_MEAN)
+    rp, ci, v = drb.gen.powerlaw_csr(m, m, alpha=alpha, hi=PREC_HI, seed=SEED + 31,
+                                     dist=drb.gen.NORMAL_ROWSCALE)
+    nnz = int(rp[-1])
+    x = drb.gen.values(m, seed=SEED + 32)
+    view = lambda vals: mp.csr_matrix_view(vals, rp, ci, (m, m))
+    A64 = mp.distributed_sparse_matrix(view(v.astype(np.float64)), 0,
+                                       distr=mp.csr_row_distribution)
+    x64 = torch.from_numpy(x.astype(np.float64)).cuda()
+    y64 = torch.empty(m, dtype=torch.float64, device="cuda")
+    A64.gemv_device(x64, y64)
+    Aabs = mp.distributed_sparse_matrix(view(np.abs(v).astype(np.float64)), 0,
+                                        distr=mp.csr_row_distribution)
+    den = torch.empty(m, dtype=torch.float64, device="cuda")
+    Aabs.gemv_device(x64.abs(), den)
+    Aabs.destroy()
+    A64.destroy()
+    den = den.clamp_min(1e-300)
+    lens = torch.from_numpy(np.diff(rp).astype(np.int64)).cuda()
+    edges = [1, 2, 5, 17, 65, 257, 1025, 1 << 62]
+    bins = [(edges[i], edges[i + 1] - 1) for i in range(len(edges) - 1)]
+    b32 = alg_bytes(m, m, nnz, 4, 4, 4, 4, 4)
+    xd = torch.from_numpy(x).cuda()
+    out = {"config": {"rows": m, "nnz": nnz, "row_len": f"zipf alpha={alpha:.4f} on "
+                      f"[1,{PREC_HI}] (mean {PREC_MEAN})", "values": "N(0,1)*10^U(-3,3) per row",
+                      "reference": "FP64 SpMV of this library (checked against the oracle "
+                                   "to 1e-12 in the tests)"}}
+    variants = [("fp32", dict(), torch.float32, 4, 4),
+                ("fp32_compensated", dict(compensated=True), torch.float32, 4, 4),
+                ("bf16", dict(storage=torch.bfloat16), torch.bfloat16, 2, 2),
+                ("bf16_f32x", dict(storage=torch.bfloat16, x_dtype=torch.float32),
+                 torch.float32, 2, 4)]
+    times = {}
+    for name, kw, xdt, vb, xb in variants:
+        A = mp.distributed_sparse_matrix(view(v), 0, distr=mp.csr_row_distribution,
+                                         autotune=True, **kw)
+        xin = xd.to(xdt)
+        y = torch.empty(m, dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            A.gemv_device(xin, y)
+        ms = statistics.mean(timed_launches(lambda: A.gemv_device(xin, y), steps, stream))
+        times[name] = ms
+        err = (y.double() - y64).abs() / den
+        per_bin = {}
+        for lo, hi in bins:
+            sel = (lens >= lo) & (lens <= hi)
+            cnt = int(sel.sum())
+            if cnt:
+                e = err[sel]
+                per_bin[f"{lo}-{hi if hi < (1 << 60) else 'max'}"] = {
+                    "rows": cnt, "max": float("%.3e" % float(e.max())),
+                    "mean": float("%.3e" % float(e.mean()))}
+        nb = alg_bytes(m, m, nnz, vb, 4, 4, xb, 4)
+        out[name] = {"ms": round(ms, 4), "GBps": round(nb / (ms * 1e-3) / 1e9, 1),
+                     "effective_fp32_GBps": round(b32 / (ms * 1e-3) / 1e9, 1),
+                     "max_rel_err": float("%.3e" % float(err.max())),
+                     "mean_rel_err": float("%.3e" % float(err.mean())),
+                     "per_row_len_bin": per_bin}
+        A.destroy()
+    out["bf16_speedup_vs_fp32"] = round(times["fp32"] / times["bf16"], 3)
+    torch.cuda.empty_cache()
+    return out
+
+
+def tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+DENSE_COUNT = 64
+DENSE_K = 32
+
+
+def dense_batch_extras(args, stream):
+    """Dense multi-RHS on the tensor cores: 64 square BF16 matrices of side
+    ~ U[256, 8192] (rows padded to a multiple of 8 elements), N(0, 1) entries,
+    32 right-hand sides column-major, FP32 accumulation and output; one
+    launch for all matrices per step (plus the one-launch X layout kernel)."""
+    import torch
+    from drb import mp
+    hbm, _ = hbm_peak()
+    tpk, tkind = tensor_peak()
+    steps = max(3, min(args.steps, 10))
+    k = DENSE_K
+    rng = np.random.default_rng(SEED + 7)
+    sides = [int(s) for s in rng.integers(256, 8193, size=DENSE_COUNT)]
+    g = torch.Generator(device="cuda").manual_seed(SEED + 8)
+    As, xs, ys = [], [], []
+    for n in sides:
+        lda = (n + 7) // 8 * 8
+        As.append(torch.empty(n, lda, device="cuda", dtype=torch.bfloat16)
+                  .normal_(generator=g))
+        xs.append(torch.randn(n * k, device="cuda", generator=g).to(torch.bfloat16))
+        ys.append(torch.empty(n * k, device="cuda"))
+    P = mp.dense_batch(As, xs, ys, k, 0, ns=sides)
+    for _ in range(3):
+        P.gemv()
+    ms = statistics.mean(timed_launches(P.gemv, steps, stream))
+    P.check()
+    abytes = sum(2 * n * n for n in sides)
+    byts = abytes + sum(2 * n * k + 4 * n * k for n in sides)
+    flops = sum(2.0 * n * n * k for n in sides)
+    gbps = byts / (ms * 1e-3) / 1e9
+    tfl = flops / (ms * 1e-3) / 1e12
+    # spot check: the largest matrix against an FP32 matmul of the same bf16 values
+    i = int(np.argmax(sides))
+    n = sides[i]
+    ref = As[i][:, :n].float() @ xs[i].float().view(k, n).t()
+    got = ys[i].view(k, n).t()
+    den = As[i][:, :n].float().abs() @ xs[i].float().abs().view(k, n).t()
+    err = float(((got - ref).abs() / den.clamp_min(1e-30)).max())
+    out = {"config": {"matrices": DENSE_COUNT, "side": "U[256,8192]", "k": k,
+                      "dtype": "bf16 in, fp32 accumulate and out",
+                      "A_GB": round(abytes / 1e9, 3)},
+           "ms": round(ms, 4), "GBps": round(gbps, 1), "frac_hbm": round(gbps / hbm, 4),
+           "tflops": round(tfl, 1), "frac_tensor": round(tfl / tpk, 4),
+           "tensor_peak_kind": tkind, "bound": "hbm",
+           "max_rel_err_vs_fp32_matmul": float("%.2e" % err),
+           "launches_per_step": 2, "kernel": "dense_tc (tcgen05.mma M=128 N=32 K=16, TMA ring)"}
+    # the same products through torch (cuBLAS), one matmul per matrix, for context
+    Xs = [x.view(k, n).t() for x, n in zip(xs, sides)]
+
+    def loop():
+        for A, X, n in zip(As, Xs, sides):
+            torch.matmul(A[:, :n], X)
+    for _ in range(2):
+        loop()
+    out["torch_matmul_loop_ms"] = round(statistics.mean(timed_launches(loop, 3, stream)), 4)
+    P.destroy()
+    del As, xs, ys, Xs
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,7 +802,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
-                    help="skip the 512-matrix batched SpMM extra")
+                    help="skip the batched extras (512 CSR matrices, 64 dense squares)")
     ap.add_argument("--rows", type=int, default=M,
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,

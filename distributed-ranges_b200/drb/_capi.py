@@ -29,6 +29,7 @@ DRB_ERR_CUDA = 4
 DRB_ERR_TIMEOUT = 5
 DRB_ERR_UNSUPPORTED = 6
 DRB_ERR_NO_DEVICE = 7
+DRB_ERR_IO = 8
 
 DRB_F32, DRB_F64, DRB_BF16 = 0, 1, 2
 DRB_I32, DRB_I64 = 0, 1
@@ -46,8 +47,15 @@ DRB_FLAG_BF16_X_F32 = 0x40
 STATUS_NAMES = {
     0: "DRB_OK", 1: "DRB_ERR_INVALID_ARG", 2: "DRB_ERR_BAD_CSR",
     3: "DRB_ERR_OOM", 4: "DRB_ERR_CUDA", 5: "DRB_ERR_TIMEOUT",
-    6: "DRB_ERR_UNSUPPORTED", 7: "DRB_ERR_NO_DEVICE",
+    6: "DRB_ERR_UNSUPPORTED", 7: "DRB_ERR_NO_DEVICE", 8: "DRB_ERR_IO",
 }
+
+
+class CsrHost(C.Structure):
+    """drb_csr_host: host CSR arrays allocated by the library."""
+    _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64),
+                ("rowptr", C.POINTER(C.c_int64)), ("colind", C.POINTER(C.c_int64)),
+                ("values", C.POINTER(C.c_double))]
 
 
 class DrbError(RuntimeError):
@@ -103,6 +111,8 @@ DRB_SYMBOLS = [
     ("drb_dense_batch_destroy", _st, [_vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_dot_noalloc", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
+    ("drb_read_matrix_market", _st, [C.c_char_p, _i32, C.POINTER(CsrHost)]),
+    ("drb_csr_host_free", None, [C.POINTER(CsrHost)]),
     ("drb_malloc", _st, [C.POINTER(_vp), C.c_size_t]),
     ("drb_free", _st, [_vp]),
     ("drb_memcpy", _st, [_vp, _vp, C.c_size_t, _i32, _vp]),

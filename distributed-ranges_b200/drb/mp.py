@@ -27,7 +27,7 @@ __all__ = [
     "csr_eq_distribution", "distributed_sparse_matrix", "broadcasted_vector",
     "broadcasted_slim_matrix", "gemv", "gemv_backward", "dense_gemv", "dot",
     "residual_norm2", "default_comm", "init", "finalize", "batch", "batched_gemv",
-    "dense_batch",
+    "dense_batch", "read_csr",
 ]
 
 _TORCH_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
@@ -115,6 +115,27 @@ class csr_matrix_view:
         for i in range(self._shape[0]):
             for p in range(int(rp[i]), int(rp[i + 1])):
                 yield (i, int(ci[p])), v[p]
+
+
+def read_csr(path, one_indexed: bool = True, dtype=np.float64, index_dtype=np.int64):
+    """dr::read_csr<T, I>(path, one_indexed) (include/dr/detail/matrix_io.hpp:
+    246-256): a coordinate Matrix Market file as a host csr_matrix_view
+    (values ``dtype``, indices ``index_dtype``), parsed by the library
+    (drb_read_matrix_market).  Raises DrbError (DRB_ERR_IO, _UNSUPPORTED or
+    _BAD_CSR) with the reference's messages."""
+    h = capi.CsrHost()
+    check(capi.lib.drb_read_matrix_market(str(path).encode(), int(one_indexed),
+                                          C.byref(h)))
+    try:
+        m, n, nnz = h.m, h.n, h.nnz
+        rp = np.ctypeslib.as_array(h.rowptr, (m + 1,)).astype(index_dtype, copy=True)
+        ci = (np.ctypeslib.as_array(h.colind, (nnz,)).astype(index_dtype, copy=True)
+              if nnz else np.zeros(0, index_dtype))
+        v = (np.ctypeslib.as_array(h.values, (nnz,)).astype(dtype, copy=True)
+             if nnz else np.zeros(0, dtype))
+    finally:
+        capi.lib.drb_csr_host_free(C.byref(h))
+    return csr_matrix_view(v, rp, ci, (m, n))
 
 
 class distribution:

@@ -19,6 +19,8 @@
  *   drb_csr_get_entries
  *       shape(), nnz(), segments() and the segment iterator's get()
  *       (distributed_sparse_matrix.hpp:141-149; csr_row_segment.hpp:140-208).
+ *   drb_read_matrix_market
+ *       dr::read_csr (include/dr/detail/matrix_io.hpp:120-256).
  *   drb_csr_gemv / drb_csr_gemv_host
  *       dr::mp::gemv(root, res, A, broadcasted_vector | broadcasted_slim_matrix)
  *       include/dr/mp/algorithms/matrix/gemv.hpp:16-39 ->
@@ -58,6 +60,7 @@ typedef int drb_status;
 #define DRB_ERR_TIMEOUT 5     /* a bounded device-side wait expired         */
 #define DRB_ERR_UNSUPPORTED 6 /* valid request this build does not handle   */
 #define DRB_ERR_NO_DEVICE 7   /* no CUDA device / wrong architecture        */
+#define DRB_ERR_IO 8          /* file missing, unreadable or not parsable   */
 
 typedef enum { DRB_F32 = 0, DRB_F64 = 1, DRB_BF16 = 2 } drb_dtype;
 typedef enum { DRB_I32 = 0, DRB_I64 = 1 } drb_itype;
@@ -276,6 +279,30 @@ drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
  * given n), though its partial sums are grouped differently. */
 drb_status drb_dot_noalloc(int64_t n, const void *a, const void *b,
                            drb_dtype dtype, double *out, void *stream);
+
+/* ---- ingest ----------------------------------------------------------------
+ * drb_read_matrix_market replaces dr::read_csr<T, I>(path, one_indexed)
+ * (include/dr/detail/matrix_io.hpp:120-256): a coordinate Matrix Market file
+ * (field real, integer or pattern -- pattern entries get value 1; symmetry
+ * general or symmetric -- off-diagonal entries of a symmetric file are stored
+ * at (i, j) and (j, i)) into host CSR arrays with rows sorted by column
+ * (entries with equal columns keep their file order).  Errors, with the
+ * reference's messages: DRB_ERR_IO (cannot open, not a coordinate Matrix
+ * Market file, malformed line), DRB_ERR_UNSUPPORTED (skew-symmetric,
+ * hermitian, ...), DRB_ERR_BAD_CSR (entry out of bounds, more entries than
+ * the size line declares; the first one in file order is reported).  Blank
+ * lines are skipped.  The arrays are allocated by the library: release them
+ * with drb_csr_host_free.  Pass the result to drb_csr_create (DRB_I64,
+ * DRB_F64) to upload it. */
+typedef struct {
+  int64_t m, n, nnz;
+  int64_t *rowptr; /* m + 1 */
+  int64_t *colind; /* nnz */
+  double *values;  /* nnz */
+} drb_csr_host;
+drb_status drb_read_matrix_market(const char *path, int one_indexed,
+                                  drb_csr_host *out);
+void drb_csr_host_free(drb_csr_host *h);
 
 /* ---- device memory (the reference's allocator and sycl_copy) --------------
  * Replaces dr::mp::__detail::allocator (include/dr/mp/allocator.hpp:14-33,

@@ -222,8 +222,34 @@ auto generate_band_csr(I size, std::size_t up_band = 3,
                                       nnz, 0);
 }
 
+// dr::read_csr<T, I>(path, one_indexed) (include/dr/detail/matrix_io.hpp:
+// 246-256): a coordinate Matrix Market file, parsed by the library
+// (drb_read_matrix_market), as a host view with arrays owned by the caller
+// (free with __detail::destroy_csr_matrix_view).  Errors throw
+// std::runtime_error with the reference's messages.
+template <typename T, typename I = std::size_t>
+auto read_csr(std::string file_path, bool one_indexed = true) {
+  drb_csr_host h{};
+  if (drb_read_matrix_market(file_path.c_str(), one_indexed ? 1 : 0, &h) !=
+      DRB_OK)
+    throw std::runtime_error(drb_last_error());
+  T *values = new T[h.nnz > 0 ? h.nnz : 1];
+  I *rowptr = new I[h.m + 1];
+  I *colind = new I[h.nnz > 0 ? h.nnz : 1];
+  for (int64_t i = 0; i <= h.m; i++)
+    rowptr[i] = (I)h.rowptr[i];
+  for (int64_t k = 0; k < h.nnz; k++) {
+    colind[k] = (I)h.colind[k];
+    values[k] = (T)h.values[k];
+  }
+  const index<I> shape((I)h.m, (I)h.n);
+  const std::size_t nnz = (std::size_t)h.nnz;
+  drb_csr_host_free(&h);
+  return views::csr_matrix_view<T, I>(values, rowptr, colind, shape, nnz, 0);
+}
+
 namespace __detail {
-// Frees a view made by the generators (matrix_io.hpp:235-243).
+// Frees a view made by the generators or read_csr (matrix_io.hpp:235-243).
 template <typename T, typename I, typename A = std::allocator<T>>
 void destroy_csr_matrix_view(views::csr_matrix_view<T, I> view, A = A{}) {
   delete[] view.values_data();

@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_GEN = os.path.join(HERE, "_ref", "ref_gen")
+REF_MMREAD = os.path.join(HERE, "_ref", "ref_mmread")
 
 F32, F64 = 0, 1
 I32, I64, U64 = 0, 1, 2
@@ -40,6 +41,11 @@ _SIGS = {
     "orc_dot": (C.c_double, [_i, _i64, _v, _v]),
     "orc_f32_to_bf16": (None, [_i64, _v, _v]),
     "orc_bf16_to_f32": (None, [_i64, _v, _v]),
+    "orc_read_matrix_market": (_i, [C.c_char_p, _i, C.POINTER(_i64), C.POINTER(_i64),
+                                    C.POINTER(_i64), C.POINTER(C.c_void_p),
+                                    C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                    C.c_char_p, _i]),
+    "orc_free": (None, [_v]),
 }
 for _n, (_r, _a) in _SIGS.items():
     _f = getattr(lib, _n)
@@ -197,3 +203,33 @@ def read_ref_bin(path):
     raw = open(path, "rb").read()
     m, n, nnz = np.frombuffer(raw[:24], np.int64)
     return int(m), int(n), int(nnz), raw[24:]
+
+
+class MatrixMarketError(RuntimeError):
+    def __init__(self, code, msg):
+        self.code = code
+        super().__init__(msg)
+
+
+def read_matrix_market(path, one_indexed=True):
+    """Restated dr::read_csr<double, long>: (m, n, rowptr, colind, values)
+    as int64 / int64 / float64 arrays; raises MatrixMarketError(code, msg)."""
+    m, n, nnz = _i64(), _i64(), _i64()
+    rp, ci, v = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    err = C.create_string_buffer(512)
+    rc = lib.orc_read_matrix_market(str(path).encode(), int(one_indexed), C.byref(m),
+                                    C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci),
+                                    C.byref(v), err, 512)
+    if rc != 0:
+        raise MatrixMarketError(rc, err.value.decode())
+    try:
+        k = nnz.value
+        rowptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(_i64)), (m.value + 1,)).copy()
+        colind = (np.ctypeslib.as_array(C.cast(ci, C.POINTER(_i64)), (k,)).copy()
+                  if k else np.zeros(0, np.int64))
+        values = (np.ctypeslib.as_array(C.cast(v, C.POINTER(C.c_double)), (k,)).copy()
+                  if k else np.zeros(0, np.float64))
+    finally:
+        for q in (rp, ci, v):
+            lib.orc_free(q)
+    return m.value, n.value, rowptr, colind, values

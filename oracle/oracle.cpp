@@ -11,6 +11,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 #include <thread>
@@ -519,5 +521,125 @@ void orc_bf16_to_f32(int64_t n, const uint16_t *in, float *out) {
     std::memcpy(&out[i], &u, 4);
   }
 }
+
+
+// ---- Matrix Market ingest --------------------------------------------------
+
+static int mm_fail(char *err, int errlen, int code, const char *msg,
+                   const char *path) {
+  if (err && errlen > 0)
+    std::snprintf(err, (size_t)errlen, "%s: %s", path, msg);
+  return code;
+}
+
+int orc_read_matrix_market(const char *path, int one_indexed, int64_t *m,
+                           int64_t *n, int64_t *nnz, int64_t **rowptr,
+                           int64_t **colind, double **values, char *err,
+                           int errlen) {
+  FILE *f = std::fopen(path, "r");
+  if (!f)
+    return mm_fail(err, errlen, 1, "mmread: cannot open", path);
+  std::vector<char> line(1 << 16);
+  auto getline = [&](void) -> bool {
+    return std::fgets(line.data(), (int)line.size(), f) != nullptr;
+  };
+  // header: five whitespace-separated tokens
+  char t[5][64] = {};
+  if (!getline() ||
+      std::sscanf(line.data(), "%63s %63s %63s %63s %63s", t[0], t[1], t[2],
+                  t[3], t[4]) < 3 ||
+      std::strcmp(t[0], "%%MatrixMarket") != 0 ||
+      std::strcmp(t[1], "matrix") != 0 || std::strcmp(t[2], "coordinate") != 0) {
+    std::fclose(f);
+    return mm_fail(err, errlen, 2, "could not be parsed as a Matrix Market file.",
+                   path);
+  }
+  const bool pattern = std::strcmp(t[3], "pattern") == 0;
+  bool symmetric;
+  if (std::strcmp(t[4], "general") == 0)
+    symmetric = false;
+  else if (std::strcmp(t[4], "symmetric") == 0)
+    symmetric = true;
+  else {
+    std::fclose(f);
+    return mm_fail(err, errlen, 3, "has an unsupported matrix type", path);
+  }
+  // comments, then the size line
+  bool have = false;
+  while (getline()) {
+    if (line[0] != '%') {
+      have = true;
+      break;
+    }
+  }
+  long long mm = 0, nn = 0, declared = 0;
+  if (!have || std::sscanf(line.data(), "%lld %lld %lld", &mm, &nn, &declared) != 3 ||
+      mm < 0 || nn < 0 || declared < 0) {
+    std::fclose(f);
+    return mm_fail(err, errlen, 6, "malformed size line", path);
+  }
+  // entries, per row in file order (mirrored entries right after theirs)
+  std::vector<std::vector<std::pair<int64_t, double>>> rows((size_t)mm);
+  long long count = 0;
+  while (getline()) {
+    const char *p = line.data();
+    while (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\n')
+      p++;
+    if (*p == 0)
+      continue; // blank line
+    long long i = 0, j = 0;
+    double v = 1.0;
+    const int got = pattern ? std::sscanf(p, "%lld %lld", &i, &j)
+                            : std::sscanf(p, "%lld %lld %lf", &i, &j, &v);
+    if (got != (pattern ? 2 : 3)) {
+      std::fclose(f);
+      return mm_fail(err, errlen, 6, "malformed entry line", path);
+    }
+    if (one_indexed) {
+      i--;
+      j--;
+    }
+    if (i < 0 || j < 0 || i >= mm || j >= nn) {
+      std::fclose(f);
+      return mm_fail(err, errlen, 4, "read_MatrixMarket: file has nonzero out of bounds.", path);
+    }
+    rows[(size_t)i].push_back({j, v});
+    if (symmetric && i != j)
+      rows[(size_t)j].push_back({i, v});
+    if (++count > declared) {
+      std::fclose(f);
+      return mm_fail(err, errlen, 5,
+                     "read_MatrixMarket: error reading Matrix Market "
+                     "file, file has more nonzeros than reported.", path);
+    }
+  }
+  std::fclose(f);
+  int64_t total = 0;
+  for (auto &r : rows) {
+    std::stable_sort(r.begin(), r.end(), [](const auto &a, const auto &b) {
+      return a.first < b.first;
+    });
+    total += (int64_t)r.size();
+  }
+  *m = mm;
+  *n = nn;
+  *nnz = total;
+  *rowptr = (int64_t *)std::malloc(sizeof(int64_t) * (size_t)(mm + 1));
+  *colind = (int64_t *)std::malloc(sizeof(int64_t) * (size_t)std::max<int64_t>(total, 1));
+  *values = (double *)std::malloc(sizeof(double) * (size_t)std::max<int64_t>(total, 1));
+  int64_t c = 0;
+  (*rowptr)[0] = 0;
+  for (int64_t r = 0; r < mm; r++) {
+    for (auto &e : rows[(size_t)r]) {
+      (*colind)[c] = e.first;
+      (*values)[c] = e.second;
+      c++;
+    }
+    (*rowptr)[r + 1] = c;
+  }
+  return 0;
+}
+
+void orc_free(void *p) { std::free(p); }
 
 } // extern "C"

@@ -122,6 +122,25 @@ double orc_dot(int vtype, int64_t n, const void *a, const void *b);
 void orc_f32_to_bf16(int64_t n, const float *in, uint16_t *out);
 void orc_bf16_to_f32(int64_t n, const uint16_t *in, float *out);
 
+/* ---- Matrix Market ingest (include/dr/detail/matrix_io.hpp) ------------ */
+
+/* Restates dr::read_csr<double, I>(path, one_indexed)
+ * (matrix_io.hpp:120-256): header "%%MatrixMarket matrix coordinate <field>
+ * <general|symmetric>" (field "pattern" gives value 1), '%' comment lines,
+ * the "m n nnz" line, then one entry per line, 1-based when one_indexed;
+ * off-diagonal entries of a symmetric file are also stored mirrored; rows are
+ * sorted by column (stable here; the reference's std::sort leaves equal
+ * columns in an unspecified order); blank lines are skipped (the reference
+ * does not handle them).  Arrays are malloc'd (free with orc_free).
+ * Returns 0, or 1 cannot open, 2 not a coordinate Matrix Market file,
+ * 3 unsupported symmetry, 4 entry out of bounds, 5 more entries than the
+ * size line declares, 6 malformed line; `err` receives a message. */
+int orc_read_matrix_market(const char *path, int one_indexed, int64_t *m,
+                           int64_t *n, int64_t *nnz, int64_t **rowptr,
+                           int64_t **colind, double **values, char *err,
+                           int errlen);
+void orc_free(void *p);
+
 #ifdef __cplusplus
 }
 #endif

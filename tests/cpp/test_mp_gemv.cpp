@@ -164,9 +164,37 @@ static int dump_random(int argc, char **argv) {
   return 0;
 }
 
+// `dump-mtx file.mtx out.bin`: dr::read_csr<double, long>(file) written in
+// oracle/_ref/ref_mmread's layout (no GPU needed); a read error prints the
+// message and returns 3, as ref_mmread does.
+static int dump_mtx(int argc, char **argv) {
+  if (argc != 4)
+    return 2;
+  try {
+    auto v = dr::read_csr<double, long>(argv[2]);
+    FILE *f = std::fopen(argv[3], "wb");
+    if (!f)
+      return 2;
+    int64_t hdr[3] = {(int64_t)v.shape()[0], (int64_t)v.shape()[1],
+                      (int64_t)v.size()};
+    std::fwrite(hdr, sizeof hdr, 1, f);
+    std::fwrite(v.rowptr_data(), sizeof(long), hdr[0] + 1, f);
+    std::fwrite(v.colind_data(), sizeof(long), hdr[2], f);
+    std::fwrite(v.values_data(), sizeof(double), hdr[2], f);
+    std::fclose(f);
+    dr::__detail::destroy_csr_matrix_view(v, std::allocator<double>{});
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return 3;
+  }
+  return 0;
+}
+
 int main(int argc, char **argv) {
   if (argc > 1 && std::string(argv[1]) == "dump-random")
     return dump_random(argc, argv);
+  if (argc > 1 && std::string(argv[1]) == "dump-mtx")
+    return dump_mtx(argc, argv);
   for (int nseg : {1, 2, 4}) {
     run_shapes<Row>("Row", nseg);
     run_shapes<Eq>("Eq", nseg);

@@ -15,6 +15,11 @@ reference tests' own rule for the expected result:
     ref[m] += n*val compared exactly (a band matrix stands in for the Matrix
     Market file, which the reference does not ship).
 
+The Matrix Market fixtures (tests/golden/mtx/*.mtx, written below) are read
+by oracle/_ref/ref_mmread, the reference's own dr::read_csr<double, long>
+(include/dr/detail/matrix_io.hpp) compiled from its source; its CSR arrays
+or its exception message are stored in mtx_<case>.npz.
+
 Run in the build container (the reference tree is needed only here):
     python tests/golden/make_golden.py
 """
@@ -29,6 +34,126 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 REF_GEN = os.path.join(ROOT, "oracle", "_ref", "ref_gen")
+REF_MMREAD = os.path.join(ROOT, "oracle", "_ref", "ref_mmread")
+MTX_DIR = os.path.join(HERE, "mtx")
+
+# Matrix Market inputs: valid files in every field/symmetry the reader takes,
+# and the malformed ones it must reject.  (No blank lines: the reference's
+# reader has no case for them.)
+MTX_CASES = {
+    "general_real": """%%MatrixMarket matrix coordinate real general
+% entries out of order, an empty row, exponents and a leading '+'
+%
+5 4 7
+3 2 1.5e-3
+1 4 -2.0
+1 1 3.25
+5 4 7
+3 1 -0.5
+1 2 1e2
+5 1 +4
+""",
+    "symmetric_real": """%%MatrixMarket matrix coordinate real symmetric
+4 4 6
+1 1 2.0
+2 1 -1.0
+2 2 2.0
+4 1 0.25
+3 3 2.0
+4 3 -1.0
+""",
+    "pattern_general": """%%MatrixMarket matrix coordinate pattern general
+3 5 5
+2 5
+1 1
+3 2
+2 1
+1 5
+""",
+    "integer_symmetric": """%%MatrixMarket matrix coordinate integer symmetric
+% integer field
+3 3 4
+1 1 7
+3 1 -2
+2 2 5
+3 2 9
+""",
+    "pattern_symmetric": """%%MatrixMarket matrix coordinate pattern symmetric
+4 4 4
+1 1
+3 1
+4 2
+4 4
+""",
+    "zero_entries": """%%MatrixMarket matrix coordinate real general
+3 3 0
+""",
+    "duplicates_equal": """%%MatrixMarket matrix coordinate real general
+2 2 4
+2 2 1.5
+1 2 3.0
+2 2 1.5
+1 1 -1.0
+""",
+    "fewer_than_declared": """%%MatrixMarket matrix coordinate real general
+3 3 5
+1 1 1.0
+3 3 3.0
+2 2 2.0
+""",
+    "tall": """%%MatrixMarket matrix coordinate real general
+6 2 5
+6 2 1.0
+1 1 2.0
+4 1 3.0
+4 2 4.0
+2 2 5.0
+""",
+    "err_array": """%%MatrixMarket matrix array real general
+2 2
+1.0
+2.0
+3.0
+4.0
+""",
+    "err_skew": """%%MatrixMarket matrix coordinate real skew-symmetric
+2 2 1
+2 1 1.0
+""",
+    "err_out_of_bounds": """%%MatrixMarket matrix coordinate real general
+3 3 2
+1 1 1.0
+4 1 1.0
+""",
+    "err_too_many": """%%MatrixMarket matrix coordinate real general
+3 3 2
+1 1 1.0
+2 2 1.0
+3 3 1.0
+""",
+    "err_not_mm": """hello
+1 1 1
+""",
+}
+
+
+def run_mmread(path):
+    out = os.path.join(HERE, "_tmp_mm.bin")
+    r = subprocess.run([REF_MMREAD, path, out], capture_output=True, text=True)
+    if r.returncode == 3:
+        return None, r.stderr.strip()
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_mmread failed on {path}: {r.returncode} {r.stderr}")
+    raw = open(out, "rb").read()
+    os.remove(out)
+    m, n, nnz = (int(v) for v in np.frombuffer(raw[:24], np.int64))
+    o = 24
+    rp = np.frombuffer(raw[o:o + 8 * (m + 1)], np.int64).copy()
+    o += 8 * (m + 1)
+    ci = np.frombuffer(raw[o:o + 8 * nnz], np.int64).copy()
+    o += 8 * nnz
+    v = np.frombuffer(raw[o:o + 8 * nnz], np.float64).copy()
+    return (m, n, rp, ci, v), None
 F32_0P1 = float(np.float32(0.1))     # the tests pass 0.1f
 F32_0P001 = float(np.float32(0.001))  # VerySparseMatrix passes 0.001f
 
@@ -122,6 +247,23 @@ def main():
     save("band_f32_100_3_3", m=mm, n=nn, rowptr=rp, colind=ci, values=v,
          x=np.ones(nn, np.float32), expected=expected_rowsum(mm, rp, v, np.float32),
          source=np.array("generate_band_csr<float,unsigned long>(100)"))
+    # --- Matrix Market ingest: the reference's read_csr<double, long>
+    if not os.path.exists(REF_MMREAD):
+        sys.exit(f"{REF_MMREAD} missing: run `make -C oracle ref` first")
+    os.makedirs(MTX_DIR, exist_ok=True)
+    for name, text in MTX_CASES.items():
+        path = os.path.join(MTX_DIR, name + ".mtx")
+        with open(path, "w") as f:
+            f.write(text)
+        res, err = run_mmread(path)
+        if res is None:
+            # the message without the path prefix
+            save("mtx_" + name, error=np.array(err.replace(path, "").strip()),
+                 source=np.array("dr::read_csr<double,long> exception"))
+        else:
+            m, n, rp, ci, v = res
+            save("mtx_" + name, m=m, n=n, rowptr=rp, colind=ci, values=v,
+                 source=np.array("dr::read_csr<double,long>"))
     # --- the other index types of the generator (same seed): int32 and long
     for it in ("i32", "i64"):
         mm, nn, rp, ci, v = run_ref(["random", "f64", it, "200", "150", repr(F32_0P1), "7"],
