@@ -286,6 +286,10 @@ def run_ours(args):
         if not args.no_batch:
             extra["batched"] = batch_extras(args, stream)
             extra["dense_batch_bf16"] = dense_batch_extras(args, stream)
+            b = extra["batched"]
+            b["effective_over_plain_fp32_spmv"] = {
+                nm: round(b["batch_" + nm]["effective_fp32_spmv_GBps"] / achieved, 2)
+                for nm in ("fp32", "bf16")}
 
     line = None
     if rank == 0:
@@ -445,9 +449,12 @@ def batch_extras(args, stream):
         byts = nnz * (4 + vb) + (rows + BATCH_COUNT) * 4 + rows * k * (xb + 4)
         gbps = byts / (ms * 1e-3) / 1e9
         rate = nnz / (ms * 1e-3)
+        # the same products as k separate plain FP32 SpMVs per matrix
+        eff = k * alg_bytes(rows, rows, nnz, 4, 4, 4, 4, 4) / (ms * 1e-3) / 1e9
         res[name] = ms
         out["batch_" + name] = {
             "ms": round(ms, 3), "GBps": round(gbps, 1), "frac": round(gbps / peak, 4),
+            "effective_fp32_spmv_GBps": round(eff, 1),
             "gflops": round(2 * nnz * k / (ms * 1e-3) / 1e9, 1),
             "gathers_per_s": round(rate / 1e9, 2),
             "gather_ceiling_frac": round(rate / ROW_GATHER_CEILING[k * xb], 4),
@@ -793,6 +800,56 @@ def dense_batch_extras(args, stream):
     return out
 
 
+def profile_case(name):
+    """A short run of one kernel on a small case of its bench workload, for
+    ncu captures (three launches after one warm-up):
+      batch16  the batched SpMM on the first 16 matrices of the 512-matrix
+               distribution (fp32, k = 16, column-major, default variant);
+      dense64  the tensor-core dense batch of the 64 BF16 squares (k = 32)."""
+    import torch
+    import drb
+    from drb import mp
+    if name == "batch16":
+        k = BATCH_K
+        rng = np.random.default_rng(SEED + 5)
+        rows = rng.integers(1024, 200001, size=BATCH_COUNT)[:16]
+        g = torch.Generator(device="cuda").manual_seed(SEED + 6)
+        mats, xs, ys = [], [], []
+        for i, m in enumerate(rows):
+            m = int(m)
+            rp, ci, v = drb.gen.uniform_rows_csr(m, m, lo=8, hi=64, seed=SEED + 1000 + i)
+            mats.append(mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, m)), 0,
+                                                     distr=mp.csr_row_distribution))
+            xs.append(torch.empty(m * k, device="cuda").uniform_(-1, 1, generator=g))
+            ys.append(torch.empty(m * k, device="cuda"))
+        b = mp.batch(mats, k, 0)
+        b.bind(xs, ys)
+        for _ in range(4):
+            b.gemv()
+        torch.cuda.synchronize()
+        b.destroy()
+    elif name == "dense64":
+        k = DENSE_K
+        rng = np.random.default_rng(SEED + 7)
+        sides = [int(s) for s in rng.integers(256, 8193, size=DENSE_COUNT)]
+        g = torch.Generator(device="cuda").manual_seed(SEED + 8)
+        As, xs, ys = [], [], []
+        for n in sides:
+            As.append(torch.empty(n, (n + 7) // 8 * 8, device="cuda", dtype=torch.bfloat16)
+                      .normal_(generator=g))
+            xs.append(torch.randn(n * k, device="cuda", generator=g).to(torch.bfloat16))
+            ys.append(torch.empty(n * k, device="cuda"))
+        P = mp.dense_batch(As, xs, ys, k, 0, ns=sides)
+        for _ in range(4):
+            P.gemv()
+        P.check()
+        P.destroy()
+    else:
+        raise SystemExit(f"unknown profile case {name}")
+    print("profile case", name, "done", flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -807,7 +864,13 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
+    ap.add_argument("--profile-case", choices=["batch16", "dense64"],
+                    help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        return profile_case(args.profile_case)
     globals()["M"] = args.rows
     globals()["N_COLS"] = args.cols
     if args.warmup < 3:

@@ -74,6 +74,7 @@ __global__ void iota_kernel(T *out, int64_t n) {
 }
 
 constexpr int kAbarNT = 256;
+constexpr int kAbarSpan = 2048; // nonzeros of a row-block tile (the plan's tile)
 
 // abar[p] = ybar[row(p)] * x[col(p)], one CTA per forward row block.
 template <class V, class CI, class RI>
@@ -82,15 +83,49 @@ __global__ void __launch_bounds__(kAbarNT)
                 const V *__restrict__ ybar, const V *__restrict__ x,
                 V *__restrict__ abar, const int2 *__restrict__ blocks,
                 const Chunk *__restrict__ chunks) {
-  __shared__ int64_t s_rp[2049];
+  __shared__ int64_t s_rp[kAbarSpan + 1];
+  __shared__ uint16_t s_row[kAbarSpan]; // row (within the block) of each nonzero
   const int2 blk = blocks[blockIdx.x];
   const uint64_t pol_x = ptx::policy_evict_last();
   if (blk.y > 0) {
+    // a tile of whole rows: rows stamp their nonzeros' row ids into shared
+    // memory, then all threads stream the nonzeros coalesced
     const int r0 = blk.x, nrows = blk.y - blk.x;
     for (int i = threadIdx.x; i <= nrows; i += kAbarNT)
       s_rp[i] = (int64_t)rowptr[r0 + i];
     __syncthreads();
     const int64_t p0 = s_rp[0], p1 = s_rp[nrows];
+    const bool stamped = p1 - p0 <= kAbarSpan && nrows <= 65536;
+    if (stamped) {
+      for (int i = threadIdx.x; i < nrows; i += kAbarNT)
+        for (int64_t p = s_rp[i]; p < s_rp[i + 1]; p++)
+          s_row[p - p0] = (uint16_t)i;
+    }
+    __syncthreads();
+    if (stamped) {
+      // all of this thread's nonzeros (at most kAbarSpan / kAbarNT) at once:
+      // column loads, then x gathers, then the products
+      constexpr int U = kAbarSpan / kAbarNT;
+      CI col[U];
+      V xv[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t p = p0 + threadIdx.x + (int64_t)u * kAbarNT;
+        col[u] = p < p1 ? colind[p] : CI(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t p = p0 + threadIdx.x + (int64_t)u * kAbarNT;
+        xv[u] = p < p1 ? ptx::ld_keep(x + col[u], pol_x) : V(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t p = p0 + threadIdx.x + (int64_t)u * kAbarNT;
+        if (p < p1)
+          abar[p] = ybar[r0 + s_row[p - p0]] * xv[u];
+      }
+      return;
+    }
     for (int64_t p = p0 + threadIdx.x; p < p1; p += kAbarNT) {
       int lo = 0, hi = nrows; // last i with s_rp[i] <= p
       while (hi - lo > 1) {

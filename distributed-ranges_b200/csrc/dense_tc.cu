@@ -290,7 +290,8 @@ __global__ void __launch_bounds__(kThreads, 1) dense_tc(const DArgs a) {
 }
 
 // Xp[j*ldp + c] = X(c, j) for c < n: the right-hand sides of every matrix
-// as K-major rows, in one launch (blockIdx.y = matrix, blockIdx.z = j).
+// as K-major rows, in one launch (blockIdx.y = matrix; a few blocks per
+// matrix loop over its k right-hand sides).
 struct RhsPack {
   const uint16_t *x;
   uint16_t *xp;
@@ -300,10 +301,10 @@ struct RhsPack {
 __global__ void pack_rhs_bf16(const RhsPack *__restrict__ packs, int k,
                               int row_major) {
   const RhsPack p = packs[blockIdx.y];
-  const int j = blockIdx.z;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < p.n;
-       c += (int64_t)gridDim.x * blockDim.x)
-    p.xp[j * p.ldp + c] = row_major ? p.x[c * k + j] : p.x[c + j * p.n];
+  for (int j = 0; j < k; j++)
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < p.n;
+         c += (int64_t)gridDim.x * blockDim.x)
+      p.xp[j * p.ldp + c] = row_major ? p.x[c * k + j] : p.x[c + j * p.n];
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -512,8 +513,8 @@ drb_status dense_batch_launch(DenseBatch &P, cudaStream_t s) {
   if (P.ntiles == 0)
     return DRB_OK;
   {
-    const dim3 grid((unsigned)std::min<int64_t>((P.max_n + 255) / 256, 64),
-                    (unsigned)P.npacks, (unsigned)P.k);
+    const dim3 grid((unsigned)std::min<int64_t>((P.max_n + 255) / 256, 8),
+                    (unsigned)P.npacks);
     pack_rhs_bf16<<<grid, 256, 0, s>>>(P.packs.as<RhsPack>(), (int)P.k,
                                        P.row_major ? 1 : 0);
     DRB_CUDA_TRY(cudaGetLastError());
