@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <thread>
 
@@ -226,7 +227,12 @@ void DevBuf::release() {
   bytes = 0;
 }
 
-Csr::~Csr() = default;
+Csr::~Csr() {
+  for (cudaEvent_t e : seg_done)
+    cudaEventDestroy(e);
+  if (copy_stream)
+    cudaStreamDestroy(copy_stream);
+}
 
 } // namespace drb
 
@@ -477,6 +483,129 @@ drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
   return spmv_launch(*A, x, y, k, layout, static_cast<cudaStream_t>(stream));
 }
 
+} // extern "C"
+
+namespace drb {
+namespace {
+
+constexpr int kHostSegments = 6;          // row segments of a host-pointer gemv
+constexpr int64_t kSegmentMinNnz = 1 << 22; // below this, one launch
+// Each segment holds this fraction of the previous one's nonzeros: y's copy
+// back over PCIe runs at about 0.6x the rate the kernel produces it, so each
+// segment's copy ends about when the next segment's compute does, and the
+// small last segment leaves a short tail.
+constexpr double kSegmentRatio = 0.6;
+
+// Segment count of a host-pointer gemv: DRB_HOST_SEGMENTS (1..64) when set,
+// read when a handle first runs one.
+int host_segments() {
+  const char *e = std::getenv("DRB_HOST_SEGMENTS");
+  if (!e || !*e)
+    return kHostSegments;
+  return std::min(64, std::max(1, std::atoi(e)));
+}
+
+// Orders the single-RHS items by row and cuts them into at most `target` row
+// segments of geometrically shrinking nnz; a chunked row never straddles two
+// segments.
+drb_status build_row_segments(Csr &A, int target) {
+  PipePlan &P = A.pipe;
+  std::vector<Item> it((size_t)P.nitems);
+  DRB_CUDA_TRY(cudaMemcpy(it.data(), P.items.p, sizeof(Item) * it.size(),
+                          cudaMemcpyDeviceToHost));
+  std::stable_sort(it.begin(), it.end(), [](const Item &a, const Item &b) {
+    return a.r0 < b.r0;
+  });
+  int64_t total = 0;
+  for (const Item &t : it)
+    total += t.len;
+  // cut[j]: running nnz at which segment j + 1 may start
+  std::vector<double> cut;
+  double w = 1.0, wsum = 0.0;
+  for (int j = 0; j < target; j++, w *= kSegmentRatio)
+    wsum += w;
+  w = 1.0;
+  for (double acc = 0.0; (int)cut.size() < target - 1; w *= kSegmentRatio) {
+    acc += w;
+    cut.push_back((double)total * acc / wsum);
+  }
+  P.seg_i0.assign(1, 0);
+  P.seg_r0.assign(1, 0);
+  int64_t acc = 0;
+  for (size_t i = 0; i < it.size(); i++) {
+    const size_t j = P.seg_i0.size() - 1;
+    // cut before item i when the running nnz passed the next target and item
+    // i starts a new row (a whole-row item, or the first chunk of its row)
+    if (i > 0 && j < cut.size() && (double)acc >= cut[j] &&
+        (it[i].nrows > 0 || it[i].r0 != it[i - 1].r0)) {
+      P.seg_i0.push_back((int64_t)i);
+      P.seg_r0.push_back(it[i].r0);
+    }
+    acc += it[i].len;
+  }
+  P.seg_i0.push_back((int64_t)it.size());
+  P.seg_r0.push_back(A.m);
+  DRB_TRY(P.seg_items.alloc(sizeof(Item) * std::max<size_t>(it.size(), 1)));
+  DRB_CUDA_TRY(cudaMemcpy(P.seg_items.p, it.data(), sizeof(Item) * it.size(),
+                          cudaMemcpyHostToDevice));
+  return DRB_OK;
+}
+
+// y = A x for one right-hand side with host x and y: x goes up, then each row
+// segment runs while the rows of the previous ones copy back on a second
+// stream.  The segment launches run the same kernel on a subset of the items,
+// so y is bit-identical to drb_csr_gemv's.
+drb_status gemv_host_segmented(Csr &A, const void *x_host, void *y_host,
+                               size_t xb, size_t yb, cudaStream_t s) {
+  PipePlan &P = A.pipe;
+  if (P.seg_i0.empty())
+    DRB_TRY(build_row_segments(A, host_segments()));
+  const int nseg = (int)P.seg_i0.size() - 1;
+  if (!A.copy_stream)
+    DRB_CUDA_TRY(cudaStreamCreateWithFlags(&A.copy_stream, cudaStreamNonBlocking));
+  while ((int)A.seg_done.size() < nseg + 1) {
+    cudaEvent_t e;
+    DRB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    A.seg_done.push_back(e);
+  }
+  DRB_CUDA_TRY(cudaMemcpyAsync(A.xh_dev.p, x_host, xb * A.n,
+                               cudaMemcpyHostToDevice, s));
+  // the kernel reads P.items / P.nitems: point them at one segment at a time
+  void *items0 = P.items.p;
+  const int64_t n0 = P.nitems;
+  drb_status st = DRB_OK;
+  // all segment launches first (a copy into pageable host memory would block
+  // this thread), then the copies, each behind its segment's event
+  for (int g = 0; g < nseg && st == DRB_OK; g++) {
+    P.items.p = P.seg_items.as<Item>() + P.seg_i0[g];
+    P.nitems = P.seg_i0[g + 1] - P.seg_i0[g];
+    st = spmv_pipe_launch(A, A.xh_dev.p, A.yh_dev.p, s);
+    P.items.p = items0;
+    P.nitems = n0;
+    if (st == DRB_OK && cudaEventRecord(A.seg_done[g], s) != cudaSuccess)
+      st = DRB_ERR_CUDA;
+  }
+  DRB_TRY(st);
+  for (int g = 0; g < nseg; g++) {
+    DRB_CUDA_TRY(cudaStreamWaitEvent(A.copy_stream, A.seg_done[g], 0));
+    const int64_t r0 = P.seg_r0[g], r1 = P.seg_r0[g + 1];
+    if (r1 > r0)
+      DRB_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(y_host) + yb * r0,
+                                   A.yh_dev.as<char>() + yb * r0,
+                                   yb * (r1 - r0), cudaMemcpyDeviceToHost,
+                                   A.copy_stream));
+  }
+  DRB_CUDA_TRY(cudaEventRecord(A.seg_done[nseg], A.copy_stream));
+  DRB_CUDA_TRY(cudaStreamWaitEvent(s, A.seg_done[nseg], 0));
+  DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  return DRB_OK;
+}
+
+} // namespace
+} // namespace drb
+
+extern "C" {
+
 drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
                              int64_t k, drb_layout layout, void *stream) {
   clear_error();
@@ -496,6 +625,8 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
   const size_t yb = (size_t)(A->storage == DRB_BF16 ? 4 : dtype_bytes(A->storage));
   DRB_TRY(A->xh_dev.ensure(xb * A->n * k));
   DRB_TRY(A->yh_dev.ensure(yb * A->m * k));
+  if (k == 1 && A->nnz >= kSegmentMinNnz && A->pipe.nitems > 0)
+    return gemv_host_segmented(*A, x_host, y_host, xb, yb, s);
   if (A->n > 0)
     DRB_CUDA_TRY(cudaMemcpyAsync(A->xh_dev.p, x_host, xb * A->n * k,
                                  cudaMemcpyHostToDevice, s));

@@ -133,6 +133,11 @@ struct PipePlan {
   DevBuf counters; // int[nsplit]
   DevBuf err;      // int: device-side error word (DRB_ERR_TIMEOUT)
   DevBuf red;      // double[grid] + int ticket: fused residual
+  // The same items ordered by row and cut into row segments (built on the
+  // first host-pointer gemv): segment s is seg_items[seg_i0[s], seg_i0[s+1])
+  // and covers rows [seg_r0[s], seg_r0[s+1]).
+  DevBuf seg_items;
+  std::vector<int64_t> seg_i0, seg_r0;
 };
 
 drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
@@ -162,8 +167,11 @@ struct Csr {
   std::unique_ptr<Csr> tr;
   DevBuf perm;
   int perm_bytes = 4;
-  // scratch for multi-RHS layout changes and host staging
+  // scratch for multi-RHS layout changes and host staging; the second stream
+  // and events overlap y's copy back with the remaining row segments
   DevBuf xs, ys, xh_dev, yh_dev;
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> seg_done;
   // host copy of rowptr (int64), filled on first drb_csr_get_entries
   std::vector<int64_t> rowptr_h;
   ~Csr();

@@ -126,6 +126,9 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
       acc -= 1.0;
     }
   }
+  plan.seg_items.release(); // the row-segment order is rebuilt on demand
+  plan.seg_i0.clear();
+  plan.seg_r0.clear();
   plan.nitems = (int64_t)all.size();
   plan.nchunks = (int64_t)chunks.size();
   plan.nsplit = nsplit;

@@ -274,6 +274,41 @@ def test_host_gemv_matches_device(mp):
     assert np.array_equal(yh.numpy(), y_dev)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("pinned", [True, False])
+def test_host_gemv_row_segments(mp, dtype, pinned):
+    """Above 4M nonzeros the host-pointer gemv runs in row segments and
+    copies each segment's rows of y back while the later ones compute; the
+    segments cut only between rows, so chunked long rows (70 000 and 300 001
+    nonzeros, placed mid-matrix) stay whole.  The result is bit-identical to
+    the device-pointer gemv, on the first call and on a repeat."""
+    rng = np.random.default_rng(31)
+    m, n = 240_000, 500_000
+    lens = rng.integers(0, 40, m)
+    lens[[1000, 120_000, 120_001, m - 1]] = [300_001, 70_000, 0, 5000]
+    rp = np.zeros(m + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    assert rp[-1] > (1 << 22)
+    rows = np.repeat(np.arange(m), lens)
+    cols = rng.integers(0, n, rp[-1])
+    ci = cols[np.lexsort((cols, rows))].astype(np.int32)
+    v = rng.uniform(-1, 1, rp[-1]).astype(dtype)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    a, y_dev = gpu_gemv(mp, rp, ci, v, m, n, x)
+    if pinned:
+        xh = torch.from_numpy(x).pin_memory().numpy()
+        yh = torch.empty(m, dtype=torch.from_numpy(x).dtype).pin_memory().numpy()
+    else:
+        xh, yh = x.copy(), np.empty(m, dtype)
+    for _ in range(2):
+        yh[:] = np.nan
+        a.gemv_host(xh, yh)
+        assert np.array_equal(yh.view(np.uint8), y_dev.view(np.uint8))
+    y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v, x, m, n)
+    assert rel_err(yh, y64, d) <= (1e-5 if dtype == np.float32 else 1e-12)
+
+
 @pytest.mark.parametrize("m,n", [(1, 1), (2, 3), (31, 33), (32, 32), (33, 31), (1, 5000)])
 def test_ragged_small_shapes(mp, m, n):
     rp, ci, v = oracle.random_csr(m, n, 0.5 if m * n > 1 else 0.0, 1, np.float64, np.int64)
