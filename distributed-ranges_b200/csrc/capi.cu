@@ -20,6 +20,7 @@ namespace drb {
 int plan_group(int vbytes, int cbytes);
 
 std::atomic<uint64_t> g_launch_count{0};
+thread_local int g_count_pause = 0;
 
 namespace {
 thread_local std::string t_error;
@@ -808,6 +809,66 @@ drb_status drb_stream_synchronize(void *stream) {
   clear_error();
   DRB_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
   return DRB_OK;
+}
+
+drb_status drb_reduce(int64_t n, const void *x, drb_dtype dtype, drb_reduce_op op,
+                      const void *init, void *out, void *stream) {
+  clear_error();
+  if (n < 0 || !out || (n > 0 && !x))
+    return invalid("NULL pointer or negative n");
+  if (!elementwise_dtype(dtype))
+    return invalid("dtype must be F32, F64, INT32 or INT64");
+  if (op != DRB_REDUCE_SUM && op != DRB_REDUCE_MIN && op != DRB_REDUCE_MAX)
+    return invalid("op must be DRB_REDUCE_SUM, _MIN or _MAX");
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  return reduce_launch(n, x, dtype, op, init, out, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_iota(int64_t n, void *x, drb_dtype dtype, int64_t start, void *stream) {
+  clear_error();
+  if (n < 0 || (n > 0 && !x))
+    return invalid("NULL pointer or negative n");
+  if (!elementwise_dtype(dtype))
+    return invalid("dtype must be F32, F64, INT32 or INT64");
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  return iota_launch(n, x, dtype, start, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_fill(int64_t n, void *x, drb_dtype dtype, const void *value, void *stream) {
+  clear_error();
+  if (n < 0 || !value || (n > 0 && !x))
+    return invalid("NULL pointer or negative n");
+  if (!elementwise_dtype(dtype))
+    return invalid("dtype must be F32, F64, INT32 or INT64");
+  int dev = 0;
+  DRB_TRY(check_device(&dev));
+  return fill_launch(n, x, dtype, value, static_cast<cudaStream_t>(stream));
+}
+
+drb_status drb_csr_cg(drb_csr_t A, const void *b, void *x, int64_t max_iters, double rtol,
+                      drb_cg_info *info, void *stream) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  if (A->m != A->n)
+    return invalid("drb_csr_cg needs a square matrix");
+  if (max_iters < 0 || !(rtol >= 0.0))
+    return invalid("max_iters < 0 or rtol not >= 0");
+  if (A->m > 0 && (!b || !x))
+    return invalid("x or b is NULL");
+  if (A->storage != DRB_F32 && A->storage != DRB_F64) {
+    set_error("drb_csr_cg: F32 or F64 storage required (BF16 storage is not supported)");
+    return DRB_ERR_UNSUPPORTED;
+  }
+  if (A->m == 0) {
+    if (info)
+      *info = drb_cg_info{0, 0.0, 0.0, 1, 0};
+    return DRB_OK;
+  }
+  DeviceGuard g(A->device);
+  return cg_solve(*A, b, x, max_iters, rtol, info, static_cast<cudaStream_t>(stream));
 }
 
 drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,

@@ -44,8 +44,14 @@ void clear_error();
 
 // Every kernel launch goes through note_launch() so the process can report
 // how many library kernels ran.
+// While a thread captures a CUDA graph it sets g_count_pause: launches
+// recorded into a graph are counted when the graph is launched.
 extern std::atomic<uint64_t> g_launch_count;
-inline void note_launch(uint64_t n = 1) { g_launch_count.fetch_add(n); }
+extern thread_local int g_count_pause;
+inline void note_launch(uint64_t n = 1) {
+  if (!g_count_pause)
+    g_launch_count.fetch_add(n);
+}
 
 // Makes `dev` current for the scope of an entry point, restoring the
 // caller's device afterwards.
@@ -138,6 +144,7 @@ struct PipePlan {
   // and covers rows [seg_r0[s], seg_r0[s+1]).
   DevBuf seg_items;
   std::vector<int64_t> seg_i0, seg_r0;
+  uint64_t gen = 0; // bumped by every (re)build
 };
 
 drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
@@ -146,6 +153,11 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
 // rowptr buffers carry this many extra zeroed elements past rowptr[m] so a
 // 16-byte-rounded bulk copy of a rowptr slice stays inside the allocation.
 constexpr int64_t kRowptrPad = 8;
+
+struct CgPlan; // conjugate-gradient workspace (cg.cu)
+struct CgPlanDeleter {
+  void operator()(CgPlan *p) const;
+};
 
 struct Csr {
   int device = 0;
@@ -172,6 +184,8 @@ struct Csr {
   DevBuf xs, ys, xh_dev, yh_dev;
   cudaStream_t copy_stream = nullptr;
   std::vector<cudaEvent_t> seg_done;
+  // conjugate-gradient workspace and its captured iteration graph
+  std::unique_ptr<CgPlan, CgPlanDeleter> cg;
   // host copy of rowptr (int64), filled on first drb_csr_get_entries
   std::vector<int64_t> rowptr_h;
   ~Csr();
@@ -188,6 +202,13 @@ drb_status spmv_t_launch(Csr &A, const void *ybar, void *xbar, cudaStream_t s);
 drb_status spmv_pipe_launch(Csr &A, const void *x, void *y, cudaStream_t s);
 drb_status residual_pipe_launch(Csr &A, const void *x, const void *b, void *y,
                                 double *out, cudaStream_t s);
+// y = A x and *out = sum_i y_i w_i (w indexed by row); returns at once when
+// *stop != 0 (stop may be null).  F32/F64 storage.
+drb_status rowdot_pipe_launch(Csr &A, const void *x, const void *w, void *y,
+                              double *out, const int *stop, cudaStream_t s);
+// Allocates (zeroed) the per-CTA partials and ticket of the fused reductions;
+// called before a graph capture so that no allocation happens inside it.
+drb_status fused_scratch(Csr &A);
 drb_status pipe_check(Csr &A, cudaStream_t s);
 drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen);
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
@@ -211,8 +232,17 @@ drb_status transpose_launch(const void *in, void *out, int64_t rows,
                             int64_t cols, int elem_bytes, cudaStream_t s);
 
 inline int dtype_bytes(drb_dtype t) {
-  return t == DRB_F64 ? 8 : (t == DRB_BF16 ? 2 : 4);
+  return (t == DRB_F64 || t == DRB_INT64) ? 8 : (t == DRB_BF16 ? 2 : 4);
 }
+
+// ---- vectors (reduce.cu) and conjugate gradients (cg.cu) ----------------------
+bool elementwise_dtype(drb_dtype t); // F32, F64, INT32, INT64
+drb_status reduce_launch(int64_t n, const void *x, drb_dtype dt, drb_reduce_op op,
+                         const void *init, void *out, cudaStream_t s);
+drb_status iota_launch(int64_t n, void *x, drb_dtype dt, int64_t start, cudaStream_t s);
+drb_status fill_launch(int64_t n, void *x, drb_dtype dt, const void *value, cudaStream_t s);
+drb_status cg_solve(Csr &A, const void *b, void *x, int64_t max_iters, double rtol,
+                    drb_cg_info *info, cudaStream_t s);
 
 } // namespace drb
 

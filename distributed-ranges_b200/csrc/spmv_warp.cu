@@ -50,6 +50,7 @@ int choose_pipe_variant(int64_t m, const void *rowptr_host, int rbytes) {
 
 drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
                            int rbytes, int group, int tile, int rows) {
+  plan.gen++; // graphs captured over the old items are stale
   if (tile == 0)
     tile = choose_pipe_variant(m, rowptr_host, rbytes);
   plan.skew = (tile & 1) != 0;
@@ -161,8 +162,22 @@ drb_status spmv_pipe_launch(Csr &A, const void *x, void *y, cudaStream_t s) {
   return DRB_ERR_UNSUPPORTED;
 }
 
-drb_status residual_pipe_launch(Csr &A, const void *x, const void *b, void *y,
-                                double *out, cudaStream_t s) {
+drb_status fused_scratch(Csr &A) {
+  PipePlan &P = A.pipe;
+  int sms = 0;
+  DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
+  const size_t bytes = sizeof(double) * ((size_t)sms * 32 + (size_t)P.nsplit) + 16;
+  if (!P.red.p || P.red.bytes < bytes) {
+    DRB_TRY(P.red.alloc(bytes));
+    DRB_CUDA_TRY(cudaMemset(P.red.p, 0, P.red.bytes));
+  }
+  return DRB_OK;
+}
+
+namespace {
+// y = A x with a fused row reduction into *out (see WarpResid).
+drb_status fused_pipe_launch(Csr &A, const void *x, const void *b, void *y, double *out,
+                             bool dot, const int *stop, cudaStream_t s) {
   PipePlan &P = A.pipe;
   if (P.nitems == 0) {
     DRB_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double), s));
@@ -171,10 +186,7 @@ drb_status residual_pipe_launch(Csr &A, const void *x, const void *b, void *y,
   int sms = 0;
   DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
   const size_t slots = (size_t)sms * 32 + (size_t)P.nsplit;
-  if (!P.red.p) {
-    DRB_TRY(P.red.alloc(sizeof(double) * slots + 16));
-    DRB_CUDA_TRY(cudaMemset(P.red.p, 0, P.red.bytes));
-  }
+  DRB_TRY(fused_scratch(A));
   WarpResid ra;
   ra.b = b;
   ra.partials = P.red.as<double>();
@@ -182,12 +194,25 @@ drb_status residual_pipe_launch(Csr &A, const void *x, const void *b, void *y,
   ra.nsplit = P.nsplit;
   ra.ticket = reinterpret_cast<int *>(P.red.as<double>() + slots);
   ra.out = out;
+  ra.stop = stop;
+  ra.dot = dot ? 1 : 0;
   if (A.storage == DRB_F32)
     return warp_launch_f32(A, x, y, &ra, false, s);
   if (A.storage == DRB_F64)
     return warp_launch_f64(A, x, y, &ra, s);
-  set_error("residual: storage type not handled");
+  set_error("fused SpMV reduction: storage type not handled");
   return DRB_ERR_UNSUPPORTED;
+}
+} // namespace
+
+drb_status residual_pipe_launch(Csr &A, const void *x, const void *b, void *y,
+                                double *out, cudaStream_t s) {
+  return fused_pipe_launch(A, x, b, y, out, false, nullptr, s);
+}
+
+drb_status rowdot_pipe_launch(Csr &A, const void *x, const void *w, void *y,
+                              double *out, const int *stop, cudaStream_t s) {
+  return fused_pipe_launch(A, x, w, y, out, true, stop, s);
 }
 
 int plan_group(int vbytes, int cbytes);

@@ -127,9 +127,13 @@ __device__ __forceinline__ Item load_item(const Item *items, int64_t i) {
 
 __device__ __forceinline__ int skew(int q) { return q + (q >> 5); }
 
-// Fused ||A x - b||^2: whole rows add into a per-CTA partial; a chunked row's
-// square goes to its own slot because which warp finishes it varies run to
-// run.  The last CTA sums partials[0..grid) then rowres[0..nsplit) in order.
+// Fused row reduction: ||A x - b||^2, or with `dot` set sum_i y_i b_i (b is
+// then a weight vector, e.g. p for p.Ap).  Whole rows add into a per-CTA
+// partial; a chunked row's term goes to its own slot because which warp
+// finishes it varies run to run.  The last CTA sums partials[0..grid) then
+// rowres[0..nsplit) in order.  A non-null `stop` pointing at a non-zero word
+// makes the whole launch return before touching anything (a converged
+// iterative loop replaying a captured graph).
 struct WarpResid {
   const void *b = nullptr;
   double *partials = nullptr;
@@ -137,6 +141,8 @@ struct WarpResid {
   int64_t nsplit = 0;
   int *ticket = nullptr;
   double *out = nullptr;
+  const int *stop = nullptr;
+  int dot = 0;
 };
 
 template <class V, class CI, int TILE> struct Slot {
@@ -217,7 +223,8 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
   // Runs the item in `sl` and refills the slot with item `refill`.
   template <bool RESID>
   __device__ __forceinline__ void process(S &sl, int64_t refill, Acc *prod, int *srp,
-                                          const Acc *bvec, double &r2, double *rowres) {
+                                          const Acc *bvec, double &r2, double *rowres,
+                                          bool dotw) {
     const Item cur = sl.d;
     const int off = (int)(cur.p0 - sl.a0), end = off + cur.len;
     const int ng = (end + G - 1) / G;
@@ -252,7 +259,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       fetch(sl, refill);
       const Acc tot = group_sum(acc.s, acc.c, 32);
       if (lane == 0)
-        finish_chunk<RESID>(cur, tot, bvec, rowres);
+        finish_chunk<RESID>(cur, tot, bvec, rowres, dotw);
       return;
     }
 #pragma unroll
@@ -307,8 +314,12 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       if (r < nrows && gl == 0) {
         y[cur.r0 + r] = tot;
         if (RESID) {
-          const double dd = (double)tot - (double)bvec[cur.r0 + r];
-          r2 += dd * dd;
+          if (dotw) {
+            r2 += (double)tot * (double)bvec[cur.r0 + r];
+          } else {
+            const double dd = (double)tot - (double)bvec[cur.r0 + r];
+            r2 += dd * dd;
+          }
         }
       }
     }
@@ -319,7 +330,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
   // adds all partials in chunk order and writes y.
   template <bool RESID>
   __device__ __forceinline__ void finish_chunk(const Item &cur, Acc tot, const Acc *bvec,
-                                               double *rowres) {
+                                               double *rowres, bool dotw) {
     const Chunk ch = chunks[cur.chunk];
     partials[cur.chunk] = tot;
     __threadfence();
@@ -339,7 +350,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       counters[ch.counter] = 0; // re-armed for the next launch
       if (RESID) {
         const double dd = (double)v - (double)bvec[ch.row];
-        rowres[ch.counter] = dd * dd;
+        rowres[ch.counter] = dotw ? (double)v * (double)bvec[ch.row] : dd * dd;
       }
     }
   }
@@ -358,6 +369,8 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ double s_red[kWarps];
   __shared__ int s_last;
 
+  if (RESID && ra.stop && *static_cast<const volatile int *>(ra.stop))
+    return; // uniform: every CTA reads the same word, written by an earlier launch
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Kern<V, XT, CI, RI, TILE, SKEW, COMP> K{rowptr, colind, vals, x, y, items, nitems,
                                       chunks, partials, counters,
@@ -373,7 +386,7 @@ __global__ void __launch_bounds__(kThreads)
   Slot<V, CI, TILE> A;
   K.fetch(A, it);
   while (A.valid) {
-    K.template process<RESID>(A, it + nw, prod, srp, bvec, r2, ra.rowres);
+    K.template process<RESID>(A, it + nw, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
     it += nw;
   }
 

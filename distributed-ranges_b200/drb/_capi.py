@@ -31,7 +31,8 @@ DRB_ERR_UNSUPPORTED = 6
 DRB_ERR_NO_DEVICE = 7
 DRB_ERR_IO = 8
 
-DRB_F32, DRB_F64, DRB_BF16 = 0, 1, 2
+DRB_F32, DRB_F64, DRB_BF16, DRB_INT32, DRB_INT64 = 0, 1, 2, 3, 4
+DRB_REDUCE_SUM, DRB_REDUCE_MIN, DRB_REDUCE_MAX = 0, 1, 2
 DRB_I32, DRB_I64 = 0, 1
 DRB_COL_MAJOR, DRB_ROW_MAJOR = 0, 1
 DRB_PART_ROW, DRB_PART_EQ = 0, 1
@@ -56,6 +57,12 @@ class CsrHost(C.Structure):
     _fields_ = [("m", C.c_int64), ("n", C.c_int64), ("nnz", C.c_int64),
                 ("rowptr", C.POINTER(C.c_int64)), ("colind", C.POINTER(C.c_int64)),
                 ("values", C.POINTER(C.c_double))]
+
+
+class CgInfo(C.Structure):
+    """drb_cg_info: how a drb_csr_cg solve ended."""
+    _fields_ = [("iterations", C.c_int64), ("residual_norm", C.c_double),
+                ("b_norm", C.c_double), ("converged", C.c_int), ("breakdown", C.c_int)]
 
 
 class DrbError(RuntimeError):
@@ -111,6 +118,10 @@ DRB_SYMBOLS = [
     ("drb_dense_batch_destroy", _st, [_vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_dot_noalloc", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
+    ("drb_reduce", _st, [_i64, _vp, _i32, _i32, _vp, _vp, _vp]),
+    ("drb_iota", _st, [_i64, _vp, _i32, _i64, _vp]),
+    ("drb_fill", _st, [_i64, _vp, _i32, _vp, _vp]),
+    ("drb_csr_cg", _st, [_vp, _vp, _vp, _i64, C.c_double, C.POINTER(CgInfo), _vp]),
     ("drb_read_matrix_market", _st, [C.c_char_p, _i32, C.POINTER(CsrHost)]),
     ("drb_csr_host_free", None, [C.POINTER(CsrHost)]),
     ("drb_malloc", _st, [C.POINTER(_vp), C.c_size_t]),

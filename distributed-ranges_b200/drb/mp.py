@@ -27,7 +27,8 @@ __all__ = [
     "csr_eq_distribution", "distributed_sparse_matrix", "broadcasted_vector",
     "broadcasted_slim_matrix", "gemv", "gemv_backward", "dense_gemv", "dot",
     "residual_norm2", "default_comm", "init", "finalize", "batch", "batched_gemv",
-    "dense_batch", "read_csr",
+    "dense_batch", "read_csr", "distributed_vector", "iota", "fill", "reduce",
+    "conjugate_gradient",
 ]
 
 _TORCH_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
@@ -632,3 +633,213 @@ def dot(a: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None,
     check(capi.lib.drb_dot(a.numel(), _ptr(a), _ptr(b), _TORCH_DT[a.dtype], _ptr(out),
                            _stream(stream)))
     return out
+
+
+# ---- distributed_vector, iota, fill, reduce --------------------------------------
+_VEC_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
+           torch.int32: capi.DRB_INT32, torch.int64: capi.DRB_INT64}
+_NP_OF = {capi.DRB_F32: np.float32, capi.DRB_F64: np.float64,
+          capi.DRB_INT32: np.int32, capi.DRB_INT64: np.int64}
+_OPS = {"plus": capi.DRB_REDUCE_SUM, "min": capi.DRB_REDUCE_MIN, "max": capi.DRB_REDUCE_MAX}
+
+
+def _op_code(op) -> int:
+    import operator
+    if op is None or op is operator.add or op is sum:
+        return capi.DRB_REDUCE_SUM
+    if op is min:
+        return capi.DRB_REDUCE_MIN
+    if op is max:
+        return capi.DRB_REDUCE_MAX
+    if isinstance(op, str) and op in _OPS:
+        return _OPS[op]
+    raise ValueError("drb: reduce supports plus (operator.add), min and max; "
+                     f"got {op!r}")
+
+
+class _VecSegment:
+    """One block of a distributed_vector: elements [begin, end) owned by
+    `rank` (dv_segment, include/dr/mp/containers/segment.hpp:214-248)."""
+
+    def __init__(self, vec: "distributed_vector", rank: int, begin: int, end: int):
+        self._vec, self._rank, self.begin, self.end = vec, rank, begin, end
+
+    def rank(self) -> int:
+        return self._rank
+
+    def size(self) -> int:
+        return self.end - self.begin
+
+    def __len__(self) -> int:
+        return self.size()
+
+    def is_local(self) -> bool:
+        return True
+
+    def data(self) -> torch.Tensor:
+        return self._vec.tensor[self.begin:self.end]
+
+
+class _Iter:
+    """Random-access position in a distributed_vector (the reference's
+    iterator: parent + offset, distributed_vector.hpp:159-230)."""
+
+    def __init__(self, vec: "distributed_vector", off: int):
+        self.vec, self.off = vec, off
+
+    def __add__(self, d: int) -> "_Iter":
+        return _Iter(self.vec, self.off + int(d))
+
+    __radd__ = __add__
+
+    def __sub__(self, d):
+        if isinstance(d, _Iter):
+            return self.off - d.off
+        return _Iter(self.vec, self.off - int(d))
+
+    def __eq__(self, o) -> bool:
+        return isinstance(o, _Iter) and o.vec is self.vec and o.off == self.off
+
+
+class distributed_vector:
+    """dr::mp::distributed_vector<T> (include/dr/mp/containers/
+    distributed_vector.hpp:150-340) on one GPU: the n elements live in one
+    device tensor; segment r holds [r*ceil(n/P), min(n, (r+1)*ceil(n/P)))
+    (segment_size, distributed_vector.hpp:310), P = nsegments.  dtype:
+    torch.float32/float64/int32/int64."""
+
+    def __init__(self, n: int, value=None, dtype=torch.float64, nsegments: int = 1,
+                 dist: distribution | None = None):
+        if n < 0 or nsegments < 1:
+            raise ValueError("drb: n must be >= 0 and nsegments >= 1")
+        if dtype not in _VEC_DT:
+            raise ValueError(f"drb: distributed_vector dtype {dtype} not supported")
+        self._n, self._P, self.dtype = int(n), int(nsegments), dtype
+        self.tensor = torch.empty(max(self._n, 1), dtype=dtype, device="cuda")[: self._n]
+        if value is not None:
+            fill(self, value)
+
+    @property
+    def code(self) -> int:
+        return _VEC_DT[self.dtype]
+
+    def size(self) -> int:
+        return self._n
+
+    def __len__(self) -> int:
+        return self._n
+
+    def segment_size(self) -> int:
+        return -(-self._n // self._P) if self._n else 0
+
+    def segments(self) -> list:
+        seg = self.segment_size()
+        return [_VecSegment(self, r, min(self._n, r * seg), min(self._n, (r + 1) * seg))
+                for r in range(self._P)]
+
+    def begin(self) -> _Iter:
+        return _Iter(self, 0)
+
+    def end(self) -> _Iter:
+        return _Iter(self, self._n)
+
+    def __getitem__(self, i: int):
+        return self.tensor[int(i)].item()
+
+    def __setitem__(self, i: int, v) -> None:
+        self.tensor[int(i)] = v
+
+    def fence(self) -> None:
+        torch.cuda.current_stream().synchronize()
+
+    def numpy(self) -> np.ndarray:
+        return self.tensor.cpu().numpy()
+
+
+def _span(r, last=None):
+    """(tensor slice, dtype code) of a vector, a segment, an iterator pair or
+    a CUDA tensor."""
+    if isinstance(r, _Iter):
+        if not isinstance(last, _Iter) or last.vec is not r.vec or last.off < r.off:
+            raise ValueError("drb: [first, last) must be iterators of one vector")
+        return r.vec.tensor[r.off:last.off], r.vec.code
+    if isinstance(r, distributed_vector):
+        return r.tensor, r.code
+    if isinstance(r, _VecSegment):
+        return r.data(), r._vec.code
+    if isinstance(r, torch.Tensor):
+        if not r.is_cuda or r.dtype not in _VEC_DT or not r.is_contiguous():
+            raise ValueError("drb: expected a contiguous CUDA tensor of f32/f64/i32/i64")
+        return r, _VEC_DT[r.dtype]
+    raise TypeError(f"drb: not a distributed range: {type(r).__name__}")
+
+
+def iota(r, value: int, last=None, stream=None) -> None:
+    """dr::mp::iota(r, value) (include/dr/mp/algorithms/iota.hpp:20-34):
+    r[i] = value + i; also iota(first, value, last) for an iterator range."""
+    t, code = _span(r, last)
+    check(capi.lib.drb_iota(t.numel(), _ptr(t), code, int(value), _stream(stream)))
+
+
+def fill(r, value, last=None, stream=None) -> None:
+    """dr::mp::fill(r, value) (include/dr/mp/algorithms/fill.hpp:21-30)."""
+    t, code = _span(r, last)
+    v = np.array([value], dtype=_NP_OF[code])
+    check(capi.lib.drb_fill(t.numel(), _ptr(t), code, C.c_void_p(v.ctypes.data),
+                            _stream(stream)))
+
+
+
+def _reduce_span(t, code, init, op, out, stream):
+    res = out if out is not None else torch.empty(1, dtype=t.dtype, device="cuda")
+    if init is not None:
+        iv = np.array([init], dtype=_NP_OF[code])
+        ip = C.c_void_p(iv.ctypes.data)
+    else:
+        ip = C.c_void_p(0)
+    check(capi.lib.drb_reduce(t.numel(), _ptr(t), code, _op_code(op), ip, _ptr(res),
+                              _stream(stream)))
+    return res if out is not None else res.item()
+
+
+def reduce(*args, out: torch.Tensor | None = None, stream=None):
+    """dr::mp::reduce (include/dr/mp/algorithms/reduce.hpp:127-181), every
+    overload: reduce(r), reduce(r, init), reduce(r, init, op),
+    reduce(root, r[, init[, op]]), and the same with an iterator pair
+    (first, last) in place of r.  op: operator.add (default), min or max --
+    the reference's std::plus and its tests' min/max lambdas.  init is
+    applied last: op(init, reduce(r)).  Returns the value on the host (root
+    0 is the only rank), or, with `out` (a 1-element CUDA tensor of the
+    element type), writes it there asynchronously and returns `out`."""
+    a = list(args)
+    if a and isinstance(a[0], (int, np.integer)) and not isinstance(a[0], bool) and \
+            len(a) > 1 and isinstance(a[1], (distributed_vector, _Iter, _VecSegment,
+                                             torch.Tensor)):
+        root = int(a.pop(0))
+        if root != 0:
+            raise ValueError("drb: root is not a rank")
+    if not a:
+        raise TypeError("drb: reduce needs a range")
+    if isinstance(a[0], _Iter):
+        t, code = _span(a[0], a[1] if len(a) > 1 else None)
+        rest = a[2:]
+    else:
+        t, code = _span(a[0])
+        rest = a[1:]
+    init = rest[0] if len(rest) > 0 else None
+    op = rest[1] if len(rest) > 1 else None
+    return _reduce_span(t, code, init, op, out, stream)
+
+
+def conjugate_gradient(a: distributed_sparse_matrix, b: torch.Tensor, x: torch.Tensor,
+                       max_iters: int = 1000, rtol: float = 1e-8, stream=None) -> dict:
+    """Solve a x = b (a symmetric positive definite, F32/F64 storage) by
+    unpreconditioned CG entirely on the GPU (drb_csr_cg); x holds the initial
+    guess and receives the solution.  Returns iterations, residual_norm,
+    b_norm, converged, breakdown."""
+    info = capi.CgInfo()
+    check(capi.lib.drb_csr_cg(a.handle, _ptr(b), _ptr(x), int(max_iters), float(rtol),
+                              C.byref(info), _stream(stream)))
+    return {"iterations": int(info.iterations), "residual_norm": float(info.residual_norm),
+            "b_norm": float(info.b_norm), "converged": bool(info.converged),
+            "breakdown": bool(info.breakdown)}

@@ -27,9 +27,15 @@
  *       local_gemv_and_collect (distributed_sparse_matrix.hpp:153-158,
  *       csr_row_distribution.hpp:137-153, csr_eq_distribution.hpp:134-153).
  *
+ *   drb_reduce / drb_iota / drb_fill
+ *       dr::mp::reduce / iota / fill over a distributed_vector
+ *       (include/dr/mp/algorithms/reduce.hpp:58-181, iota.hpp:20-34,
+ *       fill.hpp:21-30).
+ *
  * Entry points with no reference counterpart (new API shaped after gemv):
  *   drb_dense_gemv, drb_dot, drb_csr_residual_norm2, drb_csr_gemv_backward,
- *   drb_csr_update_values, drb_batch_*, drb_batched_gemv, drb_dense_batch_*.
+ *   drb_csr_update_values, drb_batch_*, drb_batched_gemv, drb_dense_batch_*,
+ *   drb_csr_cg.
  *
  * Layouts.  Multi-RHS blocks follow broadcasted_slim_matrix: column-major,
  * x[c + j*n], y[r + j*m] (gemv.hpp:29-39, csr_row_distribution.hpp:129-130).
@@ -62,7 +68,15 @@ typedef int drb_status;
 #define DRB_ERR_NO_DEVICE 7   /* no CUDA device / wrong architecture        */
 #define DRB_ERR_IO 8          /* file missing, unreadable or not parsable   */
 
-typedef enum { DRB_F32 = 0, DRB_F64 = 1, DRB_BF16 = 2 } drb_dtype;
+/* Element types.  DRB_INT32 / DRB_INT64 are accepted only by the vector
+ * entry points (drb_reduce, drb_iota, drb_fill). */
+typedef enum {
+  DRB_F32 = 0,
+  DRB_F64 = 1,
+  DRB_BF16 = 2,
+  DRB_INT32 = 3,
+  DRB_INT64 = 4
+} drb_dtype;
 typedef enum { DRB_I32 = 0, DRB_I64 = 1 } drb_itype;
 typedef enum { DRB_COL_MAJOR = 0, DRB_ROW_MAJOR = 1 } drb_layout;
 /* How the rows are split into segments (the reference's MatrixDistrT):
@@ -279,6 +293,61 @@ drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
  * given n), though its partial sums are grouped differently. */
 drb_status drb_dot_noalloc(int64_t n, const void *a, const void *b,
                            drb_dtype dtype, double *out, void *stream);
+
+/* ---- vectors: mp::reduce, iota, fill ----------------------------------------
+ * drb_reduce replaces dr::mp::reduce(root, r, init, op) / reduce(r, init, op)
+ * / reduce(r) over a distributed_vector's segments
+ * (include/dr/mp/algorithms/reduce.hpp:58-181): every segment is on this GPU,
+ * so it is one launch over x[0, n).  op is std::plus, or std::min / std::max
+ * (the reference tests' lambdas, test/gtest/common/reduce.cpp).  init: a host
+ * pointer to one element of `dtype`, applied last as op(init, reduce(x)) as
+ * reduce.hpp:110-120 does; NULL = no init.  n == 0 gives init, or zero without
+ * one (reduce.hpp:63-65, 116-118).  out: a DEVICE pointer to one element of
+ * `dtype`, written asynchronously on `stream`.  Integer sums wrap (the
+ * sequential loop's result, bit for bit); float sums accumulate in f64 and
+ * round once to dtype before init is added; min/max use std::min/std::max's
+ * comparison.  Deterministic for a given n and x % 16. */
+typedef enum {
+  DRB_REDUCE_SUM = 0,
+  DRB_REDUCE_MIN = 1,
+  DRB_REDUCE_MAX = 2
+} drb_reduce_op;
+drb_status drb_reduce(int64_t n, const void *x, drb_dtype dtype,
+                      drb_reduce_op op, const void *init, void *out,
+                      void *stream);
+/* x[i] = start + i (dr::mp::iota, include/dr/mp/algorithms/iota.hpp:20-34), and
+ * x[i] = *value (dr::mp::fill, fill.hpp:21-30; value is a host pointer to one
+ * element of dtype).  x is a device pointer; asynchronous on `stream`. */
+drb_status drb_iota(int64_t n, void *x, drb_dtype dtype, int64_t start,
+                    void *stream);
+drb_status drb_fill(int64_t n, void *x, drb_dtype dtype, const void *value,
+                    void *stream);
+
+/* ---- device-resident conjugate gradients --------------------------------------
+ * No counterpart in the reference: the loop its pieces allow (gemv + reduce +
+ * element-wise updates) run entirely on the GPU.  Solves A x = b for a
+ * symmetric positive definite A (m == n, F32 or F64 storage; x and b are
+ * device vectors of that type; x holds the initial guess on entry) with
+ * unpreconditioned CG (Hestenes-Stiefel):
+ *   r = b - A x;  p = r;  rr = r.r
+ *   repeat: q = A p;  alpha = rr / p.q;  x += alpha p;  r -= alpha q;
+ *           rr' = r.r;  stop if rr' <= rtol^2 b.b;  p = r + (rr'/rr) p
+ * The SpMV carries the p.q reduction in its epilogue; the x/r update carries
+ * r.r.  Scalars stay in device memory (f64); the loop is replayed from a
+ * CUDA graph in blocks of 8 iterations with one small device-to-host read
+ * per block, and iterations after convergence return at once.  Stops on
+ * convergence, at max_iters updates, or on breakdown (p.q <= 0 or not finite:
+ * A is not SPD; x is left as it was before that iteration).  The call
+ * synchronises `stream`. */
+typedef struct {
+  int64_t iterations;   /* updates applied to x                    */
+  double residual_norm; /* ||r|| of the recurrence at exit          */
+  double b_norm;        /* ||b||                                    */
+  int converged;        /* ||r|| <= rtol ||b||                      */
+  int breakdown;        /* p.Ap <= 0 or not finite                  */
+} drb_cg_info;
+drb_status drb_csr_cg(drb_csr_t A, const void *b, void *x, int64_t max_iters,
+                      double rtol, drb_cg_info *info, void *stream);
 
 /* ---- ingest ----------------------------------------------------------------
  * drb_read_matrix_market replaces dr::read_csr<T, I>(path, one_indexed)

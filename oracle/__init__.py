@@ -46,6 +46,9 @@ _SIGS = {
                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                     C.c_char_p, _i]),
     "orc_free": (None, [_v]),
+    "orc_cg": (_i, [_i, _i, _i64, _v, _v, _v, _v, _v, _i64, C.c_double,
+                    C.POINTER(_i64), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                    C.POINTER(_i), _v]),
 }
 for _n, (_r, _a) in _SIGS.items():
     _f = getattr(lib, _n)
@@ -233,3 +236,38 @@ def read_matrix_market(path, one_indexed=True):
         for q in (rp, ci, v):
             lib.orc_free(q)
     return m.value, n.value, rowptr, colind, values
+
+
+def cg(rp, ci, v, b, x0, max_iters, rtol, history=False):
+    """The CG restatement (orc_cg): returns (x, iterations, ||r||, ||b||,
+    status[, history]) with status 1 converged, 2 breakdown, 3 max_iters."""
+    n = len(rp) - 1
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    it, rn, bn, st = C.c_int64(), C.c_double(), C.c_double(), C.c_int()
+    hist = np.zeros(max_iters + 1) if history else None
+    assert lib.orc_cg(vcode(v.dtype), icode(ci.dtype), n, _p(rp), _p(ci), _p(v), _p(b),
+                      _p(x), max_iters, rtol, C.byref(it), C.byref(rn), C.byref(bn),
+                      C.byref(st), _p(hist)) == 0
+    out = (x, it.value, rn.value, bn.value, st.value)
+    return out + (hist[: it.value + 1],) if history else out
+
+
+def reduce_seq(x, init=None, op="plus"):
+    """std::reduce(first, last[, init], op) as the reference's tests compute
+    it (test/gtest/common/reduce.cpp): op(init, fold(x)); integer sums wrap
+    in the element type; float sums are accumulated sequentially in double
+    here (the test tolerance covers the order)."""
+    x = np.asarray(x)
+    if op == "plus":
+        if np.issubdtype(x.dtype, np.integer):
+            t = x.sum(dtype=x.dtype) if len(x) else x.dtype.type(0)
+            return t if init is None else x.dtype.type(t + x.dtype.type(init))
+        t = float(np.sum(x.astype(np.float64))) if len(x) else 0.0
+        t = x.dtype.type(t)
+        return t if init is None else x.dtype.type(x.dtype.type(init) + t)
+    f = {"min": lambda a, c: c if c < a else a, "max": lambda a, c: c if a < c else a}[op]
+    if len(x) == 0:
+        return x.dtype.type(0) if init is None else x.dtype.type(init)
+    t = x.min() if op == "min" else x.max()
+    return t if init is None else f(x.dtype.type(init), t)

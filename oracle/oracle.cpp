@@ -407,6 +407,74 @@ int orc_csr_absdot(int vtype, int itype, int64_t m, int64_t n,
   return 0;
 }
 
+int orc_cg(int vtype, int itype, int64_t n, const void *rowptr,
+           const void *colind, const void *vals, const double *b, double *x,
+           int64_t max_iters, double rtol, int64_t *iters, double *rnorm,
+           double *bnorm, int *status, double *hist) {
+  if (n < 0 || max_iters < 0)
+    return 1;
+  ORC_DISPATCH(vtype, itype, {
+    auto R = (const I *)rowptr;
+    auto Cc = (const I *)colind;
+    auto V = (const T *)vals;
+    std::vector<double> r(n), p(n), q(n);
+    auto matvec = [&](const std::vector<double> &in, std::vector<double> &out) {
+      for (int64_t i = 0; i < n; i++) {
+        double sum = 0;
+        for (int64_t k = (int64_t)R[i]; k < (int64_t)R[i + 1]; k++)
+          sum += (double)V[k] * in[(int64_t)Cc[k]];
+        out[i] = sum;
+      }
+    };
+    auto dot = [&](const std::vector<double> &a, const std::vector<double> &c) {
+      double s = 0;
+      for (int64_t i = 0; i < n; i++)
+        s += a[i] * c[i];
+      return s;
+    };
+    std::vector<double> xv(x, x + n), bv(b, b + n);
+    matvec(xv, q);
+    for (int64_t i = 0; i < n; i++)
+      r[i] = p[i] = bv[i] - q[i];
+    double rr = dot(r, r);
+    const double bb = dot(bv, bv);
+    const double tol2 = rtol * rtol * bb;
+    int64_t it = 0;
+    int st = rr <= tol2 ? 1 : (max_iters <= 0 ? 3 : 0);
+    if (hist)
+      hist[0] = std::sqrt(rr);
+    while (st == 0) {
+      matvec(p, q);
+      const double pq = dot(p, q);
+      const double alpha = rr / pq;
+      if (!(pq > 0) || !std::isfinite(alpha)) {
+        st = 2;
+        break;
+      }
+      for (int64_t i = 0; i < n; i++) {
+        xv[i] += alpha * p[i];
+        r[i] -= alpha * q[i];
+      }
+      const double rr1 = dot(r, r);
+      it++;
+      if (hist)
+        hist[it] = std::sqrt(rr1);
+      const double beta = rr1 / rr;
+      rr = rr1;
+      st = rr1 <= tol2 ? 1 : (it >= max_iters ? 3 : 0);
+      if (st == 0)
+        for (int64_t i = 0; i < n; i++)
+          p[i] = r[i] + beta * p[i];
+    }
+    std::copy(xv.begin(), xv.end(), x);
+    *iters = it;
+    *rnorm = std::sqrt(rr);
+    *bnorm = std::sqrt(bb);
+    *status = st;
+  });
+  return 0;
+}
+
 int orc_dense_gemv(int vtype, int acc, int64_t m, int64_t n, const void *A,
                    int64_t lda, const void *x, int64_t k, void *y) {
   auto run = [&](auto tag, auto acc_tag) {

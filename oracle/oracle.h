@@ -141,6 +141,26 @@ int orc_read_matrix_market(const char *path, int one_indexed, int64_t *m,
                            int errlen);
 void orc_free(void *p);
 
+/* ---- conjugate gradients (no reference symbol) ------------------------- */
+
+/* Unpreconditioned CG (Hestenes-Stiefel), all in double, built from the
+ * reference's own pieces: the product q = A p is the csr_row CPU loop
+ * (csr_row_distribution.hpp:116-133, accumulated in double) and each dot is
+ * the sequential std::reduce of zip | transform(mul) (examples/mp/
+ * dot_product_benchmark.cpp:71-79, dot_product_sequential):
+ *   r = b - A x; p = r; rr = r.r
+ *   repeat: q = A p; alpha = rr / p.q; (stop as breakdown if p.q <= 0 or
+ *           alpha not finite) x += alpha p; r -= alpha q; rr' = r.r;
+ *           stop if rr' <= rtol^2 b.b, or after max_iters updates;
+ *           p = r + (rr'/rr) p
+ * x holds the initial guess and receives the result.  status: 1 converged,
+ * 2 breakdown, 3 max_iters.  hist (may be NULL, max_iters + 1 entries):
+ * ||r|| after 0, 1, ... updates. */
+int orc_cg(int vtype, int itype, int64_t n, const void *rowptr,
+           const void *colind, const void *vals, const double *b, double *x,
+           int64_t max_iters, double rtol, int64_t *iters, double *rnorm,
+           double *bnorm, int *status, double *hist);
+
 #ifdef __cplusplus
 }
 #endif

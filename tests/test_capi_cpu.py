@@ -166,3 +166,20 @@ def test_values_distributions():
     assert abs(g.std() - 1) < 0.02
     assert np.array_equal(drb.gen.values(5000, seed=9, nthreads=1),
                           drb.gen.values(5000, seed=9, nthreads=5))
+
+
+def test_vector_and_cg_entry_points_reject_bad_arguments_without_gpu():
+    lib = capi.lib
+    out = C.c_void_p(1)
+    assert lib.drb_reduce(-1, None, capi.DRB_F32, 0, None, out, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_reduce(4, None, capi.DRB_F32, 0, None, out, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_reduce(0, None, capi.DRB_F32, 0, None, None, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_reduce(0, None, capi.DRB_BF16, 0, None, out, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_reduce(0, None, capi.DRB_INT32, 7, None, out, None) == capi.DRB_ERR_INVALID_ARG
+    assert "op" in capi.last_error()
+    assert lib.drb_iota(3, None, capi.DRB_INT64, 0, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_fill(3, out, capi.DRB_INT64, None, None) == capi.DRB_ERR_INVALID_ARG
+    assert lib.drb_fill(0, None, 9, out, None) == capi.DRB_ERR_INVALID_ARG
+    info = capi.CgInfo()
+    assert lib.drb_csr_cg(None, None, None, 10, 1e-6, C.byref(info), None) == \
+        capi.DRB_ERR_INVALID_ARG
