@@ -283,6 +283,7 @@ def run_ours(args):
         extra["config1_fixed16"] = config1_extras(args, stream)
         extra["adjoint_fd"] = adjoint_extras(args, stream)
         extra["precision"] = precision_extras(args, stream)
+        extra["cg"] = cg_extras(args, stream)
         if not args.no_batch:
             extra["batched"] = batch_extras(args, stream)
             extra["dense_batch_bf16"] = dense_batch_extras(args, stream)
@@ -588,6 +589,98 @@ def adjoint_extras(args, stream):
             A.destroy()
             del x, b, y, xbar, abar, r
         out[name] = res
+    torch.cuda.empty_cache()
+    return out
+
+
+CG_ITERS = 200
+
+
+def cg_extras(args, stream):
+    """Conjugate gradients on the 2048^2 5-point Laplacian (4,194,304 rows,
+    SPD), FP64 and FP32: CG_ITERS iterations with rtol = 0 (no early stop)
+    through drb_csr_cg, the device-resident loop (SpMV with fused p.Ap,
+    x/r update with fused r.r, p update; replayed from a CUDA graph).
+    Algorithmic bytes per iteration: the SpMV's (reference formula) + p read
+    as the dot weight + 6 vectors (update: read x, p, r, q; write x, r) + 3
+    (p update).  Beside it: the same iteration driven from the host as the
+    reference's pieces compose (gemv, then each dot returned to the host),
+    and the oracle's CPU CG (one thread) on 5 iterations, whose x after 5
+    updates is the parity check."""
+    import torch
+    import drb
+    import oracle
+    from drb import mp
+    peak, _ = hbm_peak()
+    rp, ci, v = drb.gen.laplacian2d_csr(2048, value_dtype=np.float64)
+    rp = rp.astype(np.int32)
+    m = len(rp) - 1
+    nnz = int(rp[-1])
+    g = torch.Generator(device="cuda").manual_seed(SEED + 31)
+    b64 = torch.randn(m, device="cuda", dtype=torch.float64, generator=g)
+    out = {"matrix": "laplacian2048", "rows": m, "nnz": nnz, "iterations": CG_ITERS}
+    for dt, npdt, eb in (("fp64", np.float64, 8), ("fp32", np.float32, 4)):
+        tdt = torch.float64 if dt == "fp64" else torch.float32
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v.astype(npdt), rp, ci, (m, m)), 0,
+                                         distr=mp.csr_row_distribution)
+        b = b64.to(tdt)
+        x = torch.zeros(m, device="cuda", dtype=tdt)
+        info = mp.conjugate_gradient(A, b, x, max_iters=CG_ITERS, rtol=0.0)  # captures
+        times = []
+        for _ in range(3):
+            x.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            info = mp.conjugate_gradient(A, b, x, max_iters=CG_ITERS, rtol=0.0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        it_ms = min(times) / CG_ITERS
+        ib = alg_bytes(m, m, nnz, eb, 4, 4, eb, eb) + eb * m + 6 * eb * m + 3 * eb * m
+        res = {"ms_per_iter": round(it_ms, 4), "GBps": round(ib / (it_ms * 1e-3) / 1e9, 1),
+               "frac_hbm": round(ib / (it_ms * 1e-3) / 1e9 / peak, 4),
+               "alg_bytes_per_iter": ib, "iterations_run": info["iterations"],
+               "rel_residual": float("%.3e" % (info["residual_norm"] / info["b_norm"]))}
+        # host-driven loop: gemv + dot to host per reduction (torch axpys)
+        xh = torch.zeros_like(b)
+        r = b.clone()
+        p = r.clone()
+        q = torch.empty_like(b)
+        rr = float(mp.dot(r, r).item())
+        def host_iter():
+            nonlocal rr, p
+            A.gemv_device(p, q)
+            alpha = rr / float(mp.dot(p, q).item())
+            xh.add_(p, alpha=alpha)
+            r.sub_(q, alpha=alpha)
+            rr1 = float(mp.dot(r, r).item())
+            p = r + (rr1 / rr) * p
+            rr = rr1
+        for _ in range(3):
+            host_iter()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(50):
+            host_iter()
+        torch.cuda.synchronize()
+        res["host_loop_ms_per_iter"] = round((time.perf_counter() - t0) / 50 * 1e3, 4)
+        res["device_over_host_loop"] = round(res["host_loop_ms_per_iter"] / it_ms, 2)
+        if dt == "fp64":
+            # parity: x after 5 updates against the oracle's CPU CG
+            x.zero_()
+            mp.conjugate_gradient(A, b, x, max_iters=5, rtol=0.0)
+            bh = b.cpu().numpy()
+            t0 = time.perf_counter()
+            x_o, it_o, *_ = oracle.cg(rp, ci, v, bh, np.zeros(m), 5, 0.0)
+            cpu_s = (time.perf_counter() - t0) / 5
+            xd = x.cpu().numpy()
+            res["x5_rel_diff_vs_oracle"] = float(
+                "%.3e" % (np.linalg.norm(xd - x_o) / np.linalg.norm(x_o)))
+            res["cpu_oracle_ms_per_iter_1thread"] = round(cpu_s * 1e3, 2)
+        A.destroy()
+        del x, xh, r, p, q, b
+        out[dt] = res
     torch.cuda.empty_cache()
     return out
 

@@ -774,20 +774,29 @@ def _span(r, last=None):
     raise TypeError(f"drb: not a distributed range: {type(r).__name__}")
 
 
-def iota(r, value: int, last=None, stream=None) -> None:
-    """dr::mp::iota(r, value) (include/dr/mp/algorithms/iota.hpp:20-34):
-    r[i] = value + i; also iota(first, value, last) for an iterator range."""
-    t, code = _span(r, last)
+def _range_and_value(args, name):
+    """(r, value) or (first, last, value), as the reference's overloads."""
+    if len(args) == 2:
+        return _span(args[0]), args[1]
+    if len(args) == 3:
+        return _span(args[0], args[1]), args[2]
+    raise TypeError(f"drb: {name}(r, value) or {name}(first, last, value)")
+
+
+def iota(*args, stream=None) -> None:
+    """dr::mp::iota(r, value) and iota(first, last, value)
+    (include/dr/mp/algorithms/iota.hpp:20-34): element i gets value + i."""
+    (t, code), value = _range_and_value(args, "iota")
     check(capi.lib.drb_iota(t.numel(), _ptr(t), code, int(value), _stream(stream)))
 
 
-def fill(r, value, last=None, stream=None) -> None:
-    """dr::mp::fill(r, value) (include/dr/mp/algorithms/fill.hpp:21-30)."""
-    t, code = _span(r, last)
+def fill(*args, stream=None) -> None:
+    """dr::mp::fill(r, value) and fill(first, last, value)
+    (include/dr/mp/algorithms/fill.hpp:21-30)."""
+    (t, code), value = _range_and_value(args, "fill")
     v = np.array([value], dtype=_NP_OF[code])
     check(capi.lib.drb_fill(t.numel(), _ptr(t), code, C.c_void_p(v.ctypes.data),
                             _stream(stream)))
-
 
 
 def _reduce_span(t, code, init, op, out, stream):

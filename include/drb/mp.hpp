@@ -13,6 +13,10 @@
 //   drb::mp::broadcasted_vector            .../broadcasted_vector.hpp:9-51
 //   drb::mp::broadcasted_slim_matrix       .../broadcasted_slim_matrix.hpp:9-80
 //   drb::mp::gemv (4 overloads)            include/dr/mp/algorithms/matrix/gemv.hpp:16-71
+//   drb::mp::distributed_vector            .../distributed_vector.hpp:150-340
+//   drb::mp::reduce (range and iterator    include/dr/mp/algorithms/reduce.hpp:127-232
+//     overloads), iota, fill               .../iota.hpp:20-34, .../fill.hpp:21-30
+//   drb::mp::conjugate_gradient            no reference counterpart (drb_csr_cg)
 //
 // Differences that follow from "one process owns one GPU":
 //   * default_comm() is rank 0 of 1; every segment of a matrix lives on the
@@ -649,6 +653,291 @@ template <typename T, typename I, std::ranges::output_range<T> C, typename Backe
 void gemv(C &res, distributed_sparse_matrix<T, I, Backend, MatDistr> &a,
           broadcasted_slim_matrix<T> &b) {
   gemv(0, res, a, b);
+}
+
+// ---- distributed_vector, iota, fill, reduce ---------------------------------------
+namespace detail {
+template <class T> constexpr drb_dtype vec_dtype_of() {
+  static_assert(std::is_same_v<T, float> || std::is_same_v<T, double> ||
+                    (std::is_integral_v<T> && std::is_signed_v<T> &&
+                     (sizeof(T) == 4 || sizeof(T) == 8)),
+                "distributed_vector element type: float, double, int32 or int64");
+  if constexpr (std::is_same_v<T, float>)
+    return DRB_F32;
+  else if constexpr (std::is_same_v<T, double>)
+    return DRB_F64;
+  else
+    return sizeof(T) == 4 ? DRB_INT32 : DRB_INT64;
+}
+} // namespace detail
+
+// distributed_vector<T> (distributed_vector.hpp:150-340) on one GPU: all n
+// elements in one device buffer; segment r covers [r*ceil(n/P), ...) as
+// segment_size does (distributed_vector.hpp:310), P = nsegments.  Elements
+// are read and written through get()/put() (host copies).
+template <typename T, class BackendT = MpiBackend> class distributed_vector {
+public:
+  using value_type = T;
+  using size_type = std::size_t;
+  using difference_type = std::ptrdiff_t;
+  using backend_type = BackendT;
+
+  struct segment {
+    std::size_t rank_, begin_, end_;
+    std::size_t rank() const { return rank_; }
+    std::size_t size() const { return end_ - begin_; }
+    std::size_t begin() const { return begin_; }
+    std::size_t end() const { return end_; }
+  };
+
+  class iterator {
+  public:
+    using iterator_category = std::random_access_iterator_tag;
+    using value_type = T;
+    using difference_type = std::ptrdiff_t;
+    iterator() = default;
+    iterator(const distributed_vector *p, difference_type o) : parent_(p), offset_(o) {}
+    T operator*() const { return parent_->get((std::size_t)offset_); }
+    T operator[](difference_type n) const { return *(*this + n); }
+    iterator operator+(difference_type n) const { return {parent_, offset_ + n}; }
+    friend iterator operator+(difference_type n, const iterator &it) { return it + n; }
+    iterator operator-(difference_type n) const { return {parent_, offset_ - n}; }
+    difference_type operator-(const iterator &o) const { return offset_ - o.offset_; }
+    iterator &operator+=(difference_type n) {
+      offset_ += n;
+      return *this;
+    }
+    iterator &operator-=(difference_type n) {
+      offset_ -= n;
+      return *this;
+    }
+    iterator &operator++() {
+      ++offset_;
+      return *this;
+    }
+    iterator operator++(int) {
+      auto o = *this;
+      ++offset_;
+      return o;
+    }
+    iterator &operator--() {
+      --offset_;
+      return *this;
+    }
+    iterator operator--(int) {
+      auto o = *this;
+      --offset_;
+      return o;
+    }
+    bool operator==(const iterator &o) const {
+      return parent_ == o.parent_ && offset_ == o.offset_;
+    }
+    auto operator<=>(const iterator &o) const { return offset_ <=> o.offset_; }
+    const distributed_vector *parent() const { return parent_; }
+    difference_type offset() const { return offset_; }
+
+  private:
+    const distributed_vector *parent_ = nullptr;
+    difference_type offset_ = 0;
+  };
+
+  distributed_vector(const distributed_vector &) = delete;
+  distributed_vector &operator=(const distributed_vector &) = delete;
+  explicit distributed_vector(std::size_t size = 0, distribution = distribution(),
+                              int nsegments = 1)
+      : n_(size), nseg_(std::max(1, nsegments)) {
+    buf_.allocate(size);
+  }
+  distributed_vector(std::size_t size, value_type fill_value,
+                     distribution = distribution(), int nsegments = 1)
+      : distributed_vector(size, distribution(), nsegments) {
+    check(drb_fill((int64_t)n_, buf_.data(), detail::vec_dtype_of<T>(), &fill_value,
+                   nullptr));
+  }
+
+  std::size_t size() const { return n_; }
+  iterator begin() const { return iterator(this, 0); }
+  iterator end() const { return iterator(this, (difference_type)n_); }
+  T *data() const { return buf_.data(); }
+  std::size_t segment_size() const { return (n_ + nseg_ - 1) / (std::size_t)nseg_; }
+  std::vector<segment> segments() const {
+    std::vector<segment> out;
+    const std::size_t seg = segment_size();
+    for (std::size_t r = 0; r < (std::size_t)nseg_; r++)
+      out.push_back({r, std::min(n_, r * seg), std::min(n_, (r + 1) * seg)});
+    return out;
+  }
+  T get(std::size_t i) const {
+    T v;
+    buf_.download(&v, 1, i);
+    return v;
+  }
+  void put(std::size_t i, T v) { buf_.upload(&v, 1, i); }
+  T operator[](std::size_t i) const { return get(i); }
+  void fence() { check(drb_stream_synchronize(nullptr)); }
+
+private:
+  std::size_t n_;
+  int nseg_;
+  device_buffer<T> buf_;
+};
+
+// Reduction operators the device reduce runs: std::plus, and min / max (the
+// reference tests pass min/max lambdas; name them here instead).
+namespace ops {
+struct min {
+  template <class A, class B> auto operator()(A a, B b) const { return b < a ? b : a; }
+};
+struct max {
+  template <class A, class B> auto operator()(A a, B b) const { return a < b ? b : a; }
+};
+} // namespace ops
+
+namespace detail {
+template <class O> struct is_plus : std::false_type {};
+template <class T> struct is_plus<std::plus<T>> : std::true_type {};
+template <class Op> constexpr drb_reduce_op reduce_op_of() {
+  using O = std::remove_cvref_t<Op>;
+  if constexpr (std::is_same_v<O, ops::min>)
+    return DRB_REDUCE_MIN;
+  else if constexpr (std::is_same_v<O, ops::max>)
+    return DRB_REDUCE_MAX;
+  else {
+    static_assert(is_plus<O>::value, "drb::mp::reduce runs std::plus, drb::mp::ops::min "
+                                     "or drb::mp::ops::max on the GPU");
+    return DRB_REDUCE_SUM;
+  }
+}
+
+// One reduce over [first, last) of v; the device result is copied back.
+template <class V, class Op>
+typename V::value_type reduce_span(const V &v, std::size_t first, std::size_t last,
+                                   const typename V::value_type *init, Op &&) {
+  using E = typename V::value_type;
+  device_buffer<E> out(1);
+  check(drb_reduce((int64_t)(last - first), v.data() + first, vec_dtype_of<E>(),
+                   reduce_op_of<Op>(), init, out.data(), nullptr));
+  E r;
+  out.download(&r, 1);
+  return r;
+}
+} // namespace detail
+
+// reduce over ranges (reduce.hpp:127-181) ...
+template <typename T, typename E, class B, typename Op>
+T reduce(std::size_t root, const distributed_vector<E, B> &r, T init, Op &&op) {
+  if (root != 0)
+    throw error(DRB_ERR_INVALID_ARG, "drb: root is not a rank");
+  const E i = static_cast<E>(init);
+  return static_cast<T>(detail::reduce_span(r, 0, r.size(), &i, op));
+}
+template <typename T, typename E, class B, typename Op>
+T reduce(const distributed_vector<E, B> &r, T init, Op &&op) {
+  return ::drb::mp::reduce(0, r, init, op);
+}
+template <typename T, typename E, class B>
+T reduce(std::size_t root, const distributed_vector<E, B> &r, T init) {
+  return ::drb::mp::reduce(root, r, init, std::plus<>{});
+}
+template <typename T, typename E, class B>
+T reduce(const distributed_vector<E, B> &r, T init) {
+  return ::drb::mp::reduce(0, r, init, std::plus<>{});
+}
+template <typename E, class B>
+E reduce(std::size_t root, const distributed_vector<E, B> &r) {
+  if (root != 0)
+    throw error(DRB_ERR_INVALID_ARG, "drb: root is not a rank");
+  return detail::reduce_span(r, 0, r.size(), nullptr, std::plus<>{});
+}
+template <typename E, class B> E reduce(const distributed_vector<E, B> &r) {
+  return ::drb::mp::reduce(0, r);
+}
+
+// ... and over iterator pairs (reduce.hpp:183-232).
+template <typename It, typename T, typename Op>
+  requires requires(It it) { it.parent()->data(); }
+auto reduce(std::size_t root, It first, It last, T init, Op &&op) {
+  if (root != 0)
+    throw error(DRB_ERR_INVALID_ARG, "drb: root is not a rank");
+  using V = std::remove_cvref_t<decltype(*first.parent())>;
+  using E = typename V::value_type;
+  const E i = static_cast<E>(init);
+  return static_cast<T>(detail::reduce_span(*first.parent(), (std::size_t)first.offset(),
+                                            (std::size_t)last.offset(), &i, op));
+}
+template <typename It, typename T>
+  requires requires(It it) { it.parent()->data(); }
+auto reduce(std::size_t root, It first, It last, T init) {
+  return ::drb::mp::reduce(root, first, last, init, std::plus<>{});
+}
+template <typename It>
+  requires requires(It it) { it.parent()->data(); }
+auto reduce(std::size_t root, It first, It last) {
+  if (root != 0)
+    throw error(DRB_ERR_INVALID_ARG, "drb: root is not a rank");
+  return detail::reduce_span(*first.parent(), (std::size_t)first.offset(),
+                             (std::size_t)last.offset(), nullptr, std::plus<>{});
+}
+template <typename It, typename T, typename Op>
+  requires requires(It it) { it.parent()->data(); }
+auto reduce(It first, It last, T init, Op &&op) {
+  using V = std::remove_cvref_t<decltype(*first.parent())>;
+  using E = typename V::value_type;
+  const E i = static_cast<E>(init);
+  return static_cast<T>(detail::reduce_span(*first.parent(), (std::size_t)first.offset(),
+                                            (std::size_t)last.offset(), &i, op));
+}
+template <typename It, typename T>
+  requires requires(It it) { it.parent()->data(); }
+auto reduce(It first, It last, T init) {
+  return ::drb::mp::reduce(first, last, init, std::plus<>{});
+}
+template <typename It>
+  requires requires(It it) { it.parent()->data(); }
+auto reduce(It first, It last) {
+  return detail::reduce_span(*first.parent(), (std::size_t)first.offset(),
+                             (std::size_t)last.offset(), nullptr, std::plus<>{});
+}
+
+// iota / fill (iota.hpp:20-34, fill.hpp:21-30)
+template <typename E, class B, std::integral T>
+void iota(distributed_vector<E, B> &r, T value) {
+  check(drb_iota((int64_t)r.size(), r.data(), detail::vec_dtype_of<E>(), (int64_t)value,
+                 nullptr));
+}
+template <typename It, std::integral T>
+  requires requires(It it) { it.parent()->data(); }
+void iota(It first, It last, T value) {
+  using V = std::remove_cvref_t<decltype(*first.parent())>;
+  check(drb_iota((int64_t)(last - first), first.parent()->data() + first.offset(),
+                 detail::vec_dtype_of<typename V::value_type>(), (int64_t)value, nullptr));
+}
+template <typename E, class B, typename T>
+auto fill(distributed_vector<E, B> &r, T value) {
+  const E v = static_cast<E>(value);
+  check(drb_fill((int64_t)r.size(), r.data(), detail::vec_dtype_of<E>(), &v, nullptr));
+  return r.end();
+}
+template <typename It, typename T>
+  requires requires(It it) { it.parent()->data(); }
+auto fill(It first, It last, T value) {
+  using V = std::remove_cvref_t<decltype(*first.parent())>;
+  using E = typename V::value_type;
+  const E v = static_cast<E>(value);
+  check(drb_fill((int64_t)(last - first), first.parent()->data() + first.offset(),
+                 detail::vec_dtype_of<E>(), &v, nullptr));
+  return last;
+}
+
+// ---- conjugate gradients on the device (drb_csr_cg) ------------------------------
+// Solves a x = b for symmetric positive definite a; x holds the initial guess.
+template <typename T, typename I, class B, class D>
+drb_cg_info conjugate_gradient(distributed_sparse_matrix<T, I, B, D> &a,
+                               const distributed_vector<T, B> &b, distributed_vector<T, B> &x,
+                               int64_t max_iters = 1000, double rtol = 1e-8) {
+  drb_cg_info info{};
+  check(drb_csr_cg(a.handle(), b.data(), x.data(), max_iters, rtol, &info, nullptr));
+  return info;
 }
 
 } // namespace mp

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <limits>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -141,6 +142,78 @@ void band_exact() {
   dr::__detail::destroy_csr_matrix_view(csr, std::allocator<double>{});
 }
 
+// The reference's reduce tests (test/gtest/common/reduce.cpp,
+// test/gtest/mp/reduce.cpp): Ops1 ops(10) -- a distributed_vector<int> filled
+// by iota(dist_vec, 100) -- against std::reduce on the local copy.
+void reduce_cases() {
+  dr::mp::distributed_vector<int> dv(10, dr::mp::distribution(), 3);
+  dr::mp::iota(dv, 100);
+  std::vector<int> vec(10);
+  std::iota(vec.begin(), vec.end(), 100);
+  auto mx = [](double x, double y) { return std::max(x, y); };
+  CHECK(dr::mp::reduce(0, dv, 0, std::plus{}) ==
+            std::reduce(vec.begin(), vec.end(), 0, std::plus{}),
+        "ReduceMP.RootRange");
+  CHECK(dr::mp::reduce(0, dv.begin() + 1, dv.end() - 1, 0, std::plus{}) ==
+            std::reduce(vec.begin() + 1, vec.end() - 1, 0, std::plus{}),
+        "ReduceMP.RootIterators");
+  CHECK(dr::mp::reduce(dv, 3, dr::mp::ops::max{}) == std::reduce(vec.begin(), vec.end(), 3, mx),
+        "Reduce.Range");
+  CHECK(dr::mp::reduce(dv, 3, std::plus{}) ==
+            std::reduce(vec.begin(), vec.end(), 3, std::plus{}),
+        "Reduce.Max");
+  CHECK(dr::mp::reduce(dv.begin(), dv.end(), 3, std::plus{}) ==
+            std::reduce(vec.begin(), vec.end(), 3, std::plus{}),
+        "Reduce.Iterators");
+  CHECK(dr::mp::reduce(dv, 3) == std::reduce(vec.begin(), vec.end(), 3),
+        "Reduce.RangeDefaultOp");
+  CHECK(dr::mp::reduce(dv.begin(), dv.end(), 3) == std::reduce(vec.begin(), vec.end(), 3),
+        "Reduce.IteratorsDefaultOp");
+  CHECK(dr::mp::reduce(dv) == std::reduce(vec.begin(), vec.end()), "Reduce.RangeDefaultInit");
+  CHECK(dr::mp::reduce(dv.begin(), dv.end()) == std::reduce(vec.begin(), vec.end()),
+        "Reduce.IteratorsDefaultInit");
+  // ReduceMP.TransformReduce: transform(+1) then reduce(root, ., 1, min)
+  dr::mp::distributed_vector<int> added(10);
+  dr::mp::iota(added, 101);
+  CHECK(dr::mp::reduce(0, added, 1, dr::mp::ops::min{}) == 1, "ReduceMP.TransformReduce");
+  dr::mp::fill(dv.begin() + 2, dv.end(), 7);
+  CHECK(dv[0] == 100 && dv[1] == 101 && dv[2] == 7 && dv[9] == 7, "FillIterators");
+  auto segs = dv.segments();
+  CHECK(segs.size() == 3 && segs[0].size() == 4 && segs[2].begin() == 8 && segs[2].end() == 10,
+        "VectorSegments");
+}
+
+// CG on the 1-D Laplacian tridiag(-1, 2, -1), n = 1000, b = 1.
+void cg_case() {
+  const long n = 1000;
+  std::vector<long> rp(n + 1), ci;
+  std::vector<double> v;
+  for (long i = 0; i < n; i++) {
+    rp[i] = (long)ci.size();
+    for (long j = i - 1; j <= i + 1; j++)
+      if (j >= 0 && j < n) {
+        ci.push_back(j);
+        v.push_back(j == i ? 2.0 : -1.0);
+      }
+  }
+  rp[n] = (long)ci.size();
+  dr::views::csr_matrix_view<double, long> view(v.data(), rp.data(), ci.data(),
+                                                {(long)n, (long)n}, ci.size(), 0);
+  dr::mp::distributed_sparse_matrix<double, long, dr::mp::MpiBackend,
+                                    dr::mp::csr_row_distribution<double, long>>
+      a(view, 0);
+  dr::mp::distributed_vector<double> b(n, 1.0), x(n, 0.0);
+  auto info = dr::mp::conjugate_gradient(a, b, x, 2000, 1e-10);
+  // exact solution of tridiag(-1, 2, -1) x = 1: x_i = (i+1)(n-i)/2
+  double err = 0, nx = 0;
+  for (long i = 0; i < n; i++) {
+    const double xe = 0.5 * (double)(i + 1) * (double)(n - i);
+    err = std::max(err, std::abs(x[i] - xe));
+    nx = std::max(nx, xe);
+  }
+  CHECK(info.converged && info.iterations <= n && err <= 1e-6 * nx, "ConjugateGradient1D");
+}
+
 // `dump-random m n seed out.bin`: write generate_random_csr<float, unsigned
 // long>({m, n}, 0.1f, seed) in oracle/_ref/ref_gen's layout (no GPU needed),
 // so a CPU test can compare the mirror's generator with the reference's.
@@ -202,6 +275,8 @@ int main(int argc, char **argv) {
   iter_case<Row>("Row");
   iter_case<Eq>("Eq");
   band_exact();
+  reduce_cases();
+  cg_case();
   try {
     auto bad = dr::generate_random_csr({10, 10}, 0.2f);
     bad.rowptr_data()[3] = 1000; // not monotone: rejected by the C ABI

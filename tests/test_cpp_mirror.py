@@ -74,4 +74,8 @@ def test_cpp_reference_gemv_cases(exe):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK: 0 failure(s)" in r.stdout
-    assert r.stdout.count("PASS") >= 40
+    assert r.stdout.count("PASS") >= 50
+    for case in ("ReduceMP.RootRange", "ReduceMP.RootIterators", "Reduce.Range",
+                 "Reduce.IteratorsDefaultInit", "ReduceMP.TransformReduce",
+                 "FillIterators", "VectorSegments", "ConjugateGradient1D"):
+        assert f"PASS {case}\n" in r.stdout, case

@@ -133,12 +133,14 @@ def test_iota_fill(mp, dtype):
     mp.iota(dv, start)
     want = (np.arange(n, dtype=np.int64) + start).astype(dv.numpy().dtype)
     assert np.array_equal(dv.numpy(), want)
-    mp.fill(dv.begin() + 10, 3, dv.end() - 10)
+    mp.fill(dv.begin() + 10, dv.end() - 10, 3)
     got = dv.numpy()
     assert np.array_equal(got[:10], want[:10]) and np.array_equal(got[-10:], want[-10:])
     assert (got[10:-10] == 3).all()
     v2 = mp.distributed_vector(33, value=-2, dtype=dtype)
     assert (v2.numpy() == -2).all() and v2[32] == -2
+    mp.iota(v2.begin() + 3, v2.end(), 40)
+    assert v2.numpy().tolist()[:5] == [-2, -2, -2, 40, 41] and v2[32] == 69
 
 
 def test_reduce_rejects_other_ops(mp):
