@@ -101,17 +101,156 @@ __global__ void __launch_bounds__(kDenseNT)
   }
 }
 
-template <class V, int KB, int RPW>
-void dense_call(bool vec, unsigned grid, cudaStream_t s, int64_t m, int64_t n,
-                const V *A, int64_t lda, const V *x, V *y, int64_t kbc,
-                int64_t y_ld, int64_t y_js) {
-  if (vec)
-    dense_gemv_kernel<V, KB, RPW, true><<<grid, kDenseNT, 0, s>>>(
-        m, n, A, lda, x, y, kbc, y_ld, y_js);
-  else
-    dense_gemv_kernel<V, KB, RPW, false><<<grid, kDenseNT, 0, s>>>(
-        m, n, A, lda, x, y, kbc, y_ld, y_js);
+// Balanced 16-byte path.  The work is cut into units of one row x one column
+// slab (slab_groups<V>() 16-byte groups: 32 KB of an f32 row, 16 KB of an
+// f64 row); warp w of W takes the contiguous unit range
+// [units*w/W, units*(w+1)/W), so every warp gets the same number of units
+// (+-1) whatever the shape -- tall, square or wide.  A unit's sums go to y
+// directly when a row is one slab, else to part[(row * ns + slab) * KB + j],
+// which dense_slab_sum adds in slab order (deterministic).  Each lane keeps
+// U consecutive 16-byte groups of its row in flight, so a warp reads
+// 512*U contiguous bytes per step: one row per warp with U = 4 (f32) / 16
+// (f64) measured 6.9 TB/s on 32768^2, against 4.9 TB/s (f32) for four rows
+// per warp with one group each (page locality, not occupancy, decides).
+template <class V> constexpr int64_t slab_groups() { return sizeof(V) == 4 ? 2048 : 1024; }
+template <class V, int KB> constexpr int slab_unroll() {
+  return KB == 1 ? (sizeof(V) == 4 ? 4 : 16) : (KB <= 4 ? 2 : 1);
+}
+
+template <class V, int KB>
+__global__ void __launch_bounds__(kDenseNT)
+    dense_slab_kernel(int64_t m, int64_t ng, const V *__restrict__ A, int64_t lda,
+                      const V *__restrict__ x, int64_t n, V *__restrict__ y, int64_t kbc,
+                      int64_t y_ld, int64_t y_js, V *__restrict__ part, int64_t ns,
+                      int64_t units) {
+  constexpr int PER = 16 / sizeof(V);
+  constexpr int U = slab_unroll<V, KB>();
+  constexpr int64_t SG = slab_groups<V>();
+  const uint64_t pol_s = ptx::policy_evict_first();
+  const int lane = threadIdx.x & 31;
+  const int64_t w = ((int64_t)blockIdx.x * kDenseNT + threadIdx.x) >> 5;
+  const int64_t W = ((int64_t)gridDim.x * kDenseNT) >> 5;
+  // units * W stays far below 2^63 (units <= m * n / 1024, W < 2^17)
+  const int64_t u0 = units * w / W;
+  const int64_t u1 = units * (w + 1) / W;
+  for (int64_t u = u0; u < u1; u++) {
+    const int64_t row = u / ns, sl = u - row * ns;
+    const int64_t g0 = sl * SG;
+    const int64_t g1 = min(g0 + SG, ng);
+    const V *Ar = A + row * lda;
+    V acc[KB];
+#pragma unroll
+    for (int j = 0; j < KB; j++)
+      acc[j] = 0;
+    for (int64_t gb = g0 + lane; gb < g1; gb += 32 * U) {
+      union G16 {
+        uint4 u;
+        V t[PER];
+      };
+      G16 a[U];
+#pragma unroll
+      for (int q = 0; q < U; q++) {
+        a[q].u = make_uint4(0, 0, 0, 0);
+        if (gb + 32 * q < g1)
+          a[q].u = ptx::ld_stream16(Ar + (gb + 32 * q) * PER, pol_s);
+      }
+#pragma unroll
+      for (int q = 0; q < U; q++) {
+        const int64_t g = gb + 32 * q;
+        if (g < g1) {
+#pragma unroll
+          for (int j = 0; j < KB; j++) {
+            G16 xv;
+            xv.u = __ldg(reinterpret_cast<const uint4 *>(x + j * n) + g);
+#pragma unroll
+            for (int i = 0; i < PER; i++)
+              acc[j] += a[q].t[i] * xv.t[i];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < KB; j++) {
+      const V t = warp_sum_d(acc[j]);
+      if (lane == 0 && j < kbc) {
+        if (ns == 1)
+          y[row * y_ld + j * y_js] = t;
+        else
+          part[(row * ns + sl) * KB + j] = t;
+      }
+    }
+  }
+}
+
+// y[r, j] = sum over slabs of part[(r * ns + s) * KB + j], in slab order.
+template <class V, int KB>
+__global__ void dense_slab_sum(int64_t m, int64_t ns, const V *__restrict__ part,
+                               V *__restrict__ y, int64_t kbc, int64_t y_ld, int64_t y_js) {
+  const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m * kbc; t += nth) {
+    const int64_t r = t / kbc, j = t - r * kbc;
+    const V *p = part + r * ns * KB + j;
+    V s = 0;
+    for (int64_t q = 0; q < ns; q++)
+      s += p[q * KB];
+    y[r * y_ld + j * y_js] = s;
+  }
+}
+
+template <class V, int KB>
+drb_status dense_slab_call(cudaStream_t s, int64_t m, int64_t n, const V *A, int64_t lda,
+                           const V *x, V *y, int64_t kbc, int64_t y_ld, int64_t y_js) {
+  constexpr int PER = 16 / sizeof(V);
+  constexpr int64_t SG = slab_groups<V>();
+  static int grid_cache[64] = {0};
+  int dev = 0;
+  DRB_CUDA_TRY(cudaGetDevice(&dev));
+  int &grid = grid_cache[dev < 64 ? dev : 0];
+  if (grid == 0) {
+    int occ = 0, sms = 0;
+    DRB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, dense_slab_kernel<V, KB>, kDenseNT, 0));
+    DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    grid = std::max(1, occ) * sms;
+  }
+  const int64_t ng = n / PER;
+  const int64_t ns = std::max<int64_t>(1, (ng + SG - 1) / SG);
+  const int64_t units = m * ns;
+  V *part = nullptr;
+  if (ns > 1)
+    DRB_TRY(scratch_alloc(reinterpret_cast<void **>(&part), sizeof(V) * (size_t)m * ns * KB, s));
+  const int64_t need = (units + 7) / 8; // 8 warps per CTA
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(grid, need));
+  dense_slab_kernel<V, KB><<<g, kDenseNT, 0, s>>>(m, ng, A, lda, x, n, y, kbc, y_ld, y_js,
+                                                  part, ns, units);
   note_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && ns > 1) {
+    const unsigned sg = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(148 * 16, (m * kbc + 255) / 256));
+    dense_slab_sum<V, KB><<<sg, 256, 0, s>>>(m, ns, part, y, kbc, y_ld, y_js);
+    note_launch();
+    e = cudaGetLastError();
+  }
+  if (part)
+    scratch_free(part, s);
+  if (e != cudaSuccess) {
+    set_error("dense gemv launch: %s", cudaGetErrorString(e));
+    return DRB_ERR_CUDA;
+  }
+  return DRB_OK;
+}
+
+template <class V, int KB, int RPW>
+drb_status dense_call(bool vec, unsigned grid, cudaStream_t s, int64_t m, int64_t n,
+                      const V *A, int64_t lda, const V *x, V *y, int64_t kbc,
+                      int64_t y_ld, int64_t y_js) {
+  if (vec)
+    return dense_slab_call<V, KB>(s, m, n, A, lda, x, y, kbc, y_ld, y_js);
+  dense_gemv_kernel<V, KB, RPW, false><<<grid, kDenseNT, 0, s>>>(
+      m, n, A, lda, x, y, kbc, y_ld, y_js);
+  note_launch();
+  return DRB_OK;
 }
 
 template <class V>
@@ -123,10 +262,10 @@ drb_status dense_typed(int64_t m, int64_t n, const V *A, int64_t lda,
   const V *xc = x;
   void *tmp = nullptr;
   if (layout == DRB_ROW_MAJOR && k > 1) {
-    DRB_CUDA_TRY(cudaMallocAsync(&tmp, sizeof(V) * n * k, s));
+    DRB_TRY(scratch_alloc(&tmp, sizeof(V) * n * k, s));
     drb_status st = transpose_launch(x, tmp, n, k, sizeof(V), s);
     if (st != DRB_OK) {
-      cudaFreeAsync(tmp, s);
+      scratch_free(tmp, s);
       return st;
     }
     xc = static_cast<const V *>(tmp);
@@ -142,23 +281,29 @@ drb_status dense_typed(int64_t m, int64_t n, const V *A, int64_t lda,
     const int64_t left = k - jb;
     const V *xj = xc + jb * n;
     V *yj = y + jb * y_js;
+    drb_status st;
     if (left >= 8) {
-      dense_call<V, 8, 1>(vec, grid, s, m, n, A, lda, xj, yj, 8, y_ld, y_js);
+      st = dense_call<V, 8, 1>(vec, grid, s, m, n, A, lda, xj, yj, 8, y_ld, y_js);
       jb += 8;
     } else if (left >= 4) {
-      dense_call<V, 4, 2>(vec, grid, s, m, n, A, lda, xj, yj, 4, y_ld, y_js);
+      st = dense_call<V, 4, 2>(vec, grid, s, m, n, A, lda, xj, yj, 4, y_ld, y_js);
       jb += 4;
     } else if (left >= 2) {
-      dense_call<V, 2, 2>(vec, grid, s, m, n, A, lda, xj, yj, 2, y_ld, y_js);
+      st = dense_call<V, 2, 2>(vec, grid, s, m, n, A, lda, xj, yj, 2, y_ld, y_js);
       jb += 2;
     } else {
-      dense_call<V, 1, 4>(vec, grid, s, m, n, A, lda, xj, yj, 1, y_ld, y_js);
+      st = dense_call<V, 1, 4>(vec, grid, s, m, n, A, lda, xj, yj, 1, y_ld, y_js);
       jb += 1;
+    }
+    if (st != DRB_OK) {
+      if (tmp)
+        scratch_free(tmp, s);
+      return st;
     }
   }
   cudaError_t e = cudaGetLastError();
   if (tmp)
-    cudaFreeAsync(tmp, s);
+    scratch_free(tmp, s);
   if (e != cudaSuccess) {
     set_error("dense gemv launch: %s", cudaGetErrorString(e));
     return DRB_ERR_CUDA;
@@ -331,7 +476,7 @@ drb_status dot_launch(int64_t n, const void *a, const void *b, drb_dtype dt,
   }
   void *scratch = nullptr;
   const size_t bytes = sizeof(double) * kDotGrid + 16;
-  DRB_CUDA_TRY(cudaMallocAsync(&scratch, bytes, s));
+  DRB_TRY(scratch_alloc(&scratch, bytes, s));
   double *partials = static_cast<double *>(scratch);
   int *ticket = reinterpret_cast<int *>(partials + kDotGrid);
   cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(int), s);
@@ -345,7 +490,7 @@ drb_status dot_launch(int64_t n, const void *a, const void *b, drb_dtype dt,
     note_launch();
     e = cudaGetLastError();
   }
-  cudaFreeAsync(scratch, s);
+  scratch_free(scratch, s);
   if (e != cudaSuccess) {
     set_error("dot launch: %s", cudaGetErrorString(e));
     return DRB_ERR_CUDA;

@@ -68,6 +68,11 @@ struct DeviceGuard {
   }
 };
 
+// Stream-ordered per-call scratch from a library-private pool that keeps its
+// memory mapped (util.cu); release with scratch_free on the same stream.
+drb_status scratch_alloc(void **p, size_t bytes, cudaStream_t s);
+void scratch_free(void *p, cudaStream_t s);
+
 // ---- device buffers ----------------------------------------------------------
 struct DevBuf {
   void *p = nullptr;

@@ -9,7 +9,7 @@
 // one launch: a fixed grid of kRedGrid CTAs, each thread striding over the
 // vector with 16-byte loads, a per-CTA tree, and the last CTA (completion
 // ticket) combining the per-CTA partials in index order.  The grouping
-// depends only on n, so results are deterministic.
+// depends only on n and x's address modulo 16, so results are deterministic.
 //
 // Accumulation: integer sums wrap modulo 2^32 / 2^64 (two's-complement
 // addition is associative, so the result equals the sequential loop's
@@ -163,7 +163,7 @@ drb_status reduce_typed(int64_t n, const void *x, const void *init, void *out,
     std::memcpy(&iv, init, sizeof(T));
   void *scratch = nullptr;
   const size_t bytes = sizeof(A) * kRedGrid + 16;
-  DRB_CUDA_TRY(cudaMallocAsync(&scratch, bytes, s));
+  DRB_TRY(scratch_alloc(&scratch, bytes, s));
   A *partials = static_cast<A *>(scratch);
   int *ticket = reinterpret_cast<int *>(partials + kRedGrid);
   cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(int), s);
@@ -176,7 +176,7 @@ drb_status reduce_typed(int64_t n, const void *x, const void *init, void *out,
     note_launch();
     e = cudaGetLastError();
   }
-  cudaFreeAsync(scratch, s);
+  scratch_free(scratch, s);
   if (e != cudaSuccess) {
     set_error("reduce launch: %s", cudaGetErrorString(e));
     return DRB_ERR_CUDA;

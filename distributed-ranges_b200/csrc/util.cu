@@ -1,8 +1,55 @@
 // util.cu -- small device kernels: layout transposes and element conversions
 // used at upload time and around multi-RHS calls.
+#include <cstdint>
+#include <mutex>
+
 #include "drb_internal.cuh"
 
 namespace drb {
+
+// ---- per-call scratch ------------------------------------------------------------
+// A library-private stream-ordered memory pool per device.  Its release
+// threshold keeps freed blocks mapped: the device's default pool returns
+// memory to the driver at every synchronisation, and re-mapping it on the
+// next call cost ~0.27 ms (a 32768^2 dense gemv measured 0.90 ms per call
+// against 0.63 ms of kernel time).  What the pool holds is bounded by the
+// largest scratch in flight (a few MB) and is kept until process exit.
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[64];
+} // namespace
+
+drb_status scratch_alloc(void **p, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  DRB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("scratch: device %d out of range", dev);
+    return DRB_ERR_UNSUPPORTED;
+  }
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      cudaMemPool_t created;
+      DRB_CUDA_TRY(cudaMemPoolCreate(&created, &props));
+      uint64_t keep = UINT64_MAX;
+      DRB_CUDA_TRY(cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep));
+      g_pool[dev] = created;
+    }
+    pool = g_pool[dev];
+  }
+  DRB_CUDA_TRY(cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, s));
+  return DRB_OK;
+}
+
+void scratch_free(void *p, cudaStream_t s) {
+  if (p)
+    cudaFreeAsync(p, s);
+}
 namespace {
 
 // out[c][r] = in[r][c] for a rows x cols row-major input, 32x32 smem tiles.

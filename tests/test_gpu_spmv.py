@@ -349,7 +349,11 @@ def test_gemv_size_mismatch_raises(mp):
 # ---- dense gemv, dot, fused residual ------------------------------------------
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
 @pytest.mark.parametrize("m,n,k,pad", [(257, 1024, 1, 0), (300, 777, 1, 3), (129, 512, 3, 0),
-                                       (64, 96, 8, 4), (65, 100, 9, 0), (5, 1, 1, 0)])
+                                       (64, 96, 8, 4), (65, 100, 9, 0), (5, 1, 1, 0),
+                                       # several 8 KB column slabs per row, wide and tall
+                                       (33, 5000, 1, 0), (7, 100_000, 2, 4),
+                                       (3, 1 << 20, 1, 0), (1000, 8192, 8, 0),
+                                       (1001, 4100, 5, 0), (20_000, 64, 1, 0)])
 @pytest.mark.parametrize("layout", [0, 1])
 def test_dense_gemv(mp, dtype, m, n, k, pad, layout):
     g = torch.Generator().manual_seed(m * 7 + n)
