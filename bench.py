@@ -898,7 +898,9 @@ def profile_case(name):
     ncu captures (three launches after one warm-up):
       batch16  the batched SpMM on the first 16 matrices of the 512-matrix
                distribution (fp32, k = 16, column-major, default variant);
-      dense64  the tensor-core dense batch of the 64 BF16 squares (k = 32)."""
+      dense64  the tensor-core dense batch of the 64 BF16 squares (k = 32);
+      dense_f32  the single-matrix dense gemv at 16384 x 16384 FP32 (1 GB,
+               above L2), one right-hand side."""
     import torch
     import drb
     from drb import mp
@@ -937,6 +939,14 @@ def profile_case(name):
             P.gemv()
         P.check()
         P.destroy()
+    elif name == "dense_f32":
+        g = torch.Generator(device="cuda").manual_seed(SEED + 9)
+        A = torch.randn(16384, 16384, device="cuda", generator=g)
+        x = torch.randn(16384, device="cuda", generator=g)
+        y = torch.empty(16384, device="cuda")
+        for _ in range(4):
+            mp.dense_gemv(A, x, y, 1, 0)
+        torch.cuda.synchronize()
     else:
         raise SystemExit(f"unknown profile case {name}")
     print("profile case", name, "done", flush=True)
@@ -957,7 +967,7 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
-    ap.add_argument("--profile-case", choices=["batch16", "dense64"],
+    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
