@@ -900,7 +900,9 @@ def profile_case(name):
                distribution (fp32, k = 16, column-major, default variant);
       dense64  the tensor-core dense batch of the 64 BF16 squares (k = 32);
       dense_f32  the single-matrix dense gemv at 16384 x 16384 FP32 (1 GB,
-               above L2), one right-hand side."""
+               above L2), one right-hand side;
+      laplacian_f64  the single-RHS SpMV on the 2048^2 5-point Laplacian
+               (4,194,304 rows, FP64 values, int32 indices; 335 MB)."""
     import torch
     import drb
     from drb import mp
@@ -947,6 +949,17 @@ def profile_case(name):
         for _ in range(4):
             mp.dense_gemv(A, x, y, 1, 0)
         torch.cuda.synchronize()
+    elif name == "laplacian_f64":
+        rp, ci, v = drb.gen.laplacian2d_csr(2048, value_dtype=np.float64)
+        m = len(rp) - 1
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp.astype(np.int32), ci, (m, m)),
+                                         0, distr=mp.csr_row_distribution)
+        g = torch.Generator(device="cuda").manual_seed(SEED + 10)
+        x = torch.randn(m, device="cuda", dtype=torch.float64, generator=g)
+        y = torch.empty(m, device="cuda", dtype=torch.float64)
+        for _ in range(4):
+            A.gemv_device(x, y)
+        A.check()
     else:
         raise SystemExit(f"unknown profile case {name}")
     print("profile case", name, "done", flush=True)
@@ -967,7 +980,7 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
-    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32"],
+    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:

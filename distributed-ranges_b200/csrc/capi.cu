@@ -336,6 +336,7 @@ drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
   DRB_CUDA_TRY(cudaStreamSynchronize(s));
   DRB_TRY(build_plan(A->plan, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0, 0));
   DRB_TRY(build_pipe_plan(A->pipe, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0));
+  DRB_TRY(sell_build(*A, rp_h, ib, s));
   compute_segments(*A, rp_h, ib);
   if (flags & DRB_FLAG_ADJOINT) {
     DRB_TRY(adjoint_build(*A, s));
@@ -552,6 +553,28 @@ drb_status build_row_segments(Csr &A, int target) {
   return DRB_OK;
 }
 
+// The same geometric cut for the sliced-ELL copy: slice ranges, by padded
+// elements.
+void build_slice_segments(Csr &A, int target) {
+  const std::vector<int64_t> &off = A.sell.off_h;
+  const int64_t nsl = A.sell.nslices, total = off[nsl];
+  double w = 1.0, wsum = 0.0;
+  for (int j = 0; j < target; j++, w *= kSegmentRatio)
+    wsum += w;
+  A.sell.seg_s0.assign(1, 0);
+  w = 1.0;
+  double acc = 0.0;
+  for (int j = 0; j < target - 1; j++, w *= kSegmentRatio) {
+    acc += w;
+    const double cut = (double)total * acc / wsum;
+    int64_t sl = std::lower_bound(off.begin(), off.end(), (int64_t)cut) - off.begin();
+    sl = std::min(sl, nsl);
+    if (sl > A.sell.seg_s0.back() && sl < nsl)
+      A.sell.seg_s0.push_back(sl);
+  }
+  A.sell.seg_s0.push_back(nsl);
+}
+
 // y = A x for one right-hand side with host x and y: x goes up, then each row
 // segment runs while the rows of the previous ones copy back on a second
 // stream.  The segment launches run the same kernel on a subset of the items,
@@ -559,9 +582,16 @@ drb_status build_row_segments(Csr &A, int target) {
 drb_status gemv_host_segmented(Csr &A, const void *x_host, void *y_host,
                                size_t xb, size_t yb, cudaStream_t s) {
   PipePlan &P = A.pipe;
-  if (P.seg_i0.empty())
+  const bool sell = A.sell.on;
+  if (sell && A.sell.seg_s0.empty())
+    build_slice_segments(A, host_segments());
+  if (!sell && P.seg_i0.empty())
     DRB_TRY(build_row_segments(A, host_segments()));
-  const int nseg = (int)P.seg_i0.size() - 1;
+  const int nseg = sell ? (int)A.sell.seg_s0.size() - 1 : (int)P.seg_i0.size() - 1;
+  // rows of segment g: [row0(g), row0(g + 1))
+  auto row0 = [&](int g) -> int64_t {
+    return sell ? std::min(A.m, A.sell.seg_s0[g] * 32) : P.seg_r0[g];
+  };
   if (!A.copy_stream)
     DRB_CUDA_TRY(cudaStreamCreateWithFlags(&A.copy_stream, cudaStreamNonBlocking));
   while ((int)A.seg_done.size() < nseg + 1) {
@@ -578,18 +608,23 @@ drb_status gemv_host_segmented(Csr &A, const void *x_host, void *y_host,
   // all segment launches first (a copy into pageable host memory would block
   // this thread), then the copies, each behind its segment's event
   for (int g = 0; g < nseg && st == DRB_OK; g++) {
-    P.items.p = P.seg_items.as<Item>() + P.seg_i0[g];
-    P.nitems = P.seg_i0[g + 1] - P.seg_i0[g];
-    st = spmv_pipe_launch(A, A.xh_dev.p, A.yh_dev.p, s);
-    P.items.p = items0;
-    P.nitems = n0;
+    if (sell) {
+      st = sell_launch(A, A.xh_dev.p, A.yh_dev.p, nullptr, A.sell.seg_s0[g],
+                       A.sell.seg_s0[g + 1], s);
+    } else {
+      P.items.p = P.seg_items.as<Item>() + P.seg_i0[g];
+      P.nitems = P.seg_i0[g + 1] - P.seg_i0[g];
+      st = spmv_pipe_launch(A, A.xh_dev.p, A.yh_dev.p, s);
+      P.items.p = items0;
+      P.nitems = n0;
+    }
     if (st == DRB_OK && cudaEventRecord(A.seg_done[g], s) != cudaSuccess)
       st = DRB_ERR_CUDA;
   }
   DRB_TRY(st);
   for (int g = 0; g < nseg; g++) {
     DRB_CUDA_TRY(cudaStreamWaitEvent(A.copy_stream, A.seg_done[g], 0));
-    const int64_t r0 = P.seg_r0[g], r1 = P.seg_r0[g + 1];
+    const int64_t r0 = row0(g), r1 = row0(g + 1);
     if (r1 > r0)
       DRB_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(y_host) + yb * r0,
                                    A.yh_dev.as<char>() + yb * r0,
@@ -626,7 +661,7 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
   const size_t yb = (size_t)(A->storage == DRB_BF16 ? 4 : dtype_bytes(A->storage));
   DRB_TRY(A->xh_dev.ensure(xb * A->n * k));
   DRB_TRY(A->yh_dev.ensure(yb * A->m * k));
-  if (k == 1 && A->nnz >= kSegmentMinNnz && A->pipe.nitems > 0)
+  if (k == 1 && A->nnz >= kSegmentMinNnz && (A->pipe.nitems > 0 || A->sell.on))
     return gemv_host_segmented(*A, x_host, y_host, xb, yb, s);
   if (A->n > 0)
     DRB_CUDA_TRY(cudaMemcpyAsync(A->xh_dev.p, x_host, xb * A->n * k,
@@ -674,7 +709,7 @@ drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
 drb_status drb_csr_variant(drb_csr_t A, int *variant) {
   if (!A || !variant)
     return invalid("NULL argument");
-  *variant = A->pipe.tile | (A->pipe.skew ? 1 : 0);
+  *variant = A->sell.on ? kVariantSell : A->pipe.tile | (A->pipe.skew ? 1 : 0);
   return DRB_OK;
 }
 
@@ -717,6 +752,7 @@ drb_status drb_csr_update_values(drb_csr_t A, const void *values,
   DRB_CUDA_TRY(cudaMemcpyAsync(A->vals.p, values,
                                (size_t)dtype_bytes(A->storage) * A->nnz,
                                cudaMemcpyDeviceToDevice, s));
+  DRB_TRY(sell_pack_values(*A, s));
   return adjoint_refresh_values(*A, s);
 }
 

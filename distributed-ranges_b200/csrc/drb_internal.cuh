@@ -159,6 +159,21 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
 // 16-byte-rounded bulk copy of a rowptr slice stays inside the allocation.
 constexpr int64_t kRowptrPad = 8;
 
+// Sliced-ELL copy of a matrix with short, regular rows (sell.cu): slices of
+// 32 rows, slice s padded to its longest row and stored k-major at
+// off[s] + 32*k + lane.  `on` routes the single-right-hand-side entry points
+// (gemv, fused residual, conjugate gradients) to it.
+struct Sell {
+  bool built = false, on = false;
+  int64_t nslices = 0, padded = 0;
+  int maxw = 0;
+  DevBuf vals, cols, off;            // V[padded], int32[padded], int64[nslices+1]
+  std::vector<int64_t> off_h;        // host copy of off
+  std::vector<int64_t> seg_s0;       // slice cuts of the host-pointer gemv
+};
+
+constexpr int kVariantSell = 2048; // drb_csr_variant code of the sliced-ELL kernel
+
 struct CgPlan; // conjugate-gradient workspace (cg.cu)
 struct CgPlanDeleter {
   void operator()(CgPlan *p) const;
@@ -176,6 +191,7 @@ struct Csr {
   DevBuf rowptr, colind, vals;
   Plan plan;      // row blocks: multi-RHS kernel and abar
   PipePlan pipe;  // work items: the persistent single-RHS kernel
+  Sell sell;      // sliced-ELL copy for short regular rows (when eligible)
   std::vector<int64_t> seg_row0, seg_row1, seg_nz0, seg_nz1;
   // adjoint plan: A^T as a CSR matrix of shape n x m (colptr, rowidx, values
   // in column order, its own row-block plan) and perm[nnz] (CSC position ->
@@ -215,6 +231,18 @@ drb_status rowdot_pipe_launch(Csr &A, const void *x, const void *w, void *y,
 // called before a graph capture so that no allocation happens inside it.
 drb_status fused_scratch(Csr &A);
 drb_status pipe_check(Csr &A, cudaStream_t s);
+// Builds A.sell from the host rowptr when the rows are short and regular
+// (longest <= 64, padding <= 20%, memory to spare); otherwise leaves it off.
+drb_status sell_build(Csr &A, const void *rowptr_host, int rbytes, cudaStream_t s);
+void sell_release(Csr &A);
+drb_status sell_pack_values(Csr &A, cudaStream_t s); // after the CSR values change
+namespace warpk {
+struct WarpResid;
+}
+// The sliced-ELL kernel over slices [s0, s1), with the row-block kernel's
+// fused row reduction contract when ra is given.
+drb_status sell_launch(Csr &A, const void *x, void *y, const warpk::WarpResid *ra,
+                       int64_t s0, int64_t s1, cudaStream_t s);
 drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen);
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
                        cudaStream_t s);

@@ -150,6 +150,8 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
 }
 
 drb_status spmv_pipe_launch(Csr &A, const void *x, void *y, cudaStream_t s) {
+  if (A.sell.on)
+    return sell_launch(A, x, y, nullptr, 0, A.sell.nslices, s);
   switch (A.storage) {
   case DRB_F32:
     return warp_launch_f32(A, x, y, nullptr, (A.flags & DRB_FLAG_COMPENSATED) != 0, s);
@@ -196,6 +198,8 @@ drb_status fused_pipe_launch(Csr &A, const void *x, const void *b, void *y, doub
   ra.out = out;
   ra.stop = stop;
   ra.dot = dot ? 1 : 0;
+  if (A.sell.on)
+    return sell_launch(A, x, y, &ra, 0, A.sell.nslices, s);
   if (A.storage == DRB_F32)
     return warp_launch_f32(A, x, y, &ra, false, s);
   if (A.storage == DRB_F64)
@@ -217,9 +221,10 @@ drb_status rowdot_pipe_launch(Csr &A, const void *x, const void *w, void *y,
 
 int plan_group(int vbytes, int cbytes);
 
-// Times the four single-RHS variants on this matrix's sparsity pattern (x = 0,
-// three launches each after one warm-up) and rebuilds the plan with the
-// fastest.  Returns the chosen variant (tile | skew) in *chosen.
+// Times the four single-RHS row-block variants, and the sliced-ELL copy when
+// the matrix qualifies for one, on this matrix's sparsity pattern (x = 0,
+// three launches each after one warm-up) and keeps the fastest.  Returns the
+// chosen variant (tile | skew, or kVariantSell) in *chosen.
 drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
   const int vb = dtype_bytes(A.storage);
   const int group = plan_group(vb, A.cbytes);
@@ -233,12 +238,19 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
   cudaEvent_t e0, e1;
   DRB_CUDA_TRY(cudaEventCreate(&e0));
   DRB_CUDA_TRY(cudaEventCreate(&e1));
-  const int variants[4] = {256 | 1, 256, 512 | 1, 512};
-  int best = variants[0];
-  float best_ms = 3.4e38f;
+  // the row-block variants, then the sliced-ELL copy when the rows allow one
+  if (!A.sell.built)
+    DRB_TRY(sell_build(A, rp.data(), A.rbytes, s));
+  const int variants[5] = {256 | 1, 256, 512 | 1, 512, kVariantSell};
+  const int nvar = A.sell.built ? 5 : 4;
+  int best = variants[0], best_rb = variants[0];
+  float best_ms = 3.4e38f, best_rb_ms = 3.4e38f;
   drb_status st = DRB_OK;
-  for (int v : variants) {
-    st = build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, v, 0);
+  for (int iv = 0; iv < nvar; iv++) {
+    const int v = variants[iv];
+    A.sell.on = v == kVariantSell;
+    if (!A.sell.on)
+      st = build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, v, 0);
     if (st != DRB_OK)
       break;
     if ((st = spmv_pipe_launch(A, xb.p, yb.p, s)) != DRB_OK)
@@ -255,11 +267,20 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
       best_ms = ms;
       best = v;
     }
+    if (v != kVariantSell && ms < best_rb_ms) {
+      best_rb_ms = ms;
+      best_rb = v;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   DRB_TRY(st);
-  DRB_TRY(build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, best, 0));
+  A.sell.on = best == kVariantSell;
+  // the row-block plan stays built (the multi-RHS and adjoint paths use it);
+  // its rebuild also marks captured graphs stale
+  DRB_TRY(build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, best_rb, 0));
+  if (!A.sell.on)
+    sell_release(A);
   if (chosen)
     *chosen = best;
   return DRB_OK;

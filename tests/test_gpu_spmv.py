@@ -494,3 +494,98 @@ def test_launch_count_increases(mp):
     c0 = _capi.launch_count()
     mp.gemv(0, np.zeros(100, np.float32), a, b)
     assert _capi.launch_count() == c0 + 1
+
+
+# ---- sliced-ELL copy for short, regular rows ---------------------------------------
+def stencil_like(m, n, seed, dtype):
+    """Rows of 3-5 nonzeros (mostly 5) with a few empty rows, columns near the
+    diagonal plus one far band, as a 2-D stencil has."""
+    rng = np.random.default_rng(seed)
+    lens = rng.choice([3, 4, 5], size=m, p=[0.05, 0.15, 0.8])
+    lens[[7 % m, m // 2, m - 1]] = 0
+    rp = np.zeros(m + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    rows = np.repeat(np.arange(m), lens)
+    k = np.arange(rp[-1]) - np.repeat(rp[:-1], lens)
+    off = np.array([-300, -1, 0, 1, 300])[k]
+    ci = np.clip(rows + off, 0, n - 1).astype(np.int32)
+    v = rng.uniform(-1, 1, rp[-1]).astype(dtype)
+    return rp.astype(np.int32), ci, v
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("m", [1000, 100_003, 1_000_000])
+def test_sell_short_rows_match_oracle_and_row_blocks(mp, dtype, m, monkeypatch):
+    rp, ci, v = stencil_like(m, m, m, dtype)
+    x = np.random.default_rng(1).uniform(-1, 1, m).astype(dtype)
+    a, y = gpu_gemv(mp, rp, ci, v, m, m, x)
+    assert a.variant() == 2048                      # the sliced-ELL kernel runs
+    y64 = oracle.gemv_row(rp, ci, v, x, m, m, 1, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v, x, m, m)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert rel_err(y, y64, d) <= tol
+    assert (y[[7 % m, m // 2, m - 1]] == 0).all()  # empty rows
+    monkeypatch.setenv("DRB_SPMV_VARIANT", "256,1")  # the row-block kernel
+    b, y2 = gpu_gemv(mp, rp, ci, v, m, m, x)
+    assert b.variant() == 257
+    assert rel_err(y, y2.astype(np.float64), d) <= 2 * tol
+
+
+def test_sell_not_taken_for_irregular_rows(mp):
+    rp, ci, v, m, n = chunky_matrix(np.float32)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    assert a.variant() != 2048
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_sell_fused_residual_and_value_update(mp, dtype):
+    m = 200_001
+    rp, ci, v = stencil_like(m, m, 9, dtype)
+    rng = np.random.default_rng(10)
+    x = rng.uniform(-1, 1, m).astype(dtype)
+    b = rng.uniform(-1, 1, m).astype(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, m)), 0)
+    assert a.variant() == 2048
+    xt, bt = torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda()
+    yt = torch.empty_like(xt)
+    r2 = float(mp.residual_norm2(a, xt, bt, yt).item())
+    y64 = oracle.gemv_row(rp, ci, v, x, m, m, 1, oracle.ACC_LD)
+    want = float(np.sum((y64 - b.astype(np.float64)) ** 2))
+    assert abs(r2 - want) <= (1e-4 if dtype == np.float32 else 1e-10) * want
+    # new values reach the sliced copy
+    v2 = (v * -2.5).astype(dtype)
+    a.update_values(torch.from_numpy(v2).cuda())
+    a.gemv_device(xt, yt)
+    y2 = oracle.gemv_row(rp, ci, v2, x, m, m, 1, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v2, x, m, m)
+    assert rel_err(yt.cpu().numpy(), y2, d) <= (1e-5 if dtype == np.float32 else 1e-12)
+
+
+def test_sell_host_gemv_segments_bit_identical(mp):
+    import drb
+    rp, ci, v = drb.gen.laplacian2d_csr(2048, value_dtype=np.float64)
+    m = len(rp) - 1
+    assert rp[-1] > (1 << 22)                       # the segmented host path
+    x = np.random.default_rng(11).standard_normal(m)
+    a, y_dev = gpu_gemv(mp, rp.astype(np.int32), ci, v, m, m, x)
+    assert a.variant() == 2048
+    xh = torch.from_numpy(x).pin_memory().numpy()
+    yh = torch.empty(m, dtype=torch.float64).pin_memory().numpy()
+    for _ in range(2):
+        yh[:] = np.nan
+        a.gemv_host(xh, yh)
+        assert np.array_equal(yh.view(np.uint8), y_dev.view(np.uint8))
+
+
+def test_sell_autotune_keeps_a_valid_choice(mp):
+    m = 300_000
+    rp, ci, v = stencil_like(m, m, 12, np.float64)
+    x = np.random.default_rng(13).standard_normal(m)
+    a, y = gpu_gemv(mp, rp, ci, v, m, m, x)
+    chosen = a.autotune()
+    assert chosen == a.variant() and chosen in (256, 257, 512, 513, 2048)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.empty_like(xt)
+    a.gemv_device(xt, yt)
+    y64 = oracle.gemv_row(rp, ci, v, x, m, m, 1, oracle.ACC_LD)
+    assert rel_err(yt.cpu().numpy(), y64, oracle.absdot(rp, ci, v, x, m, m)) <= 1e-12
