@@ -246,6 +246,9 @@ drb_status build_typed(Csr &A, cudaStream_t s) {
                      plan_group(dtype_bytes(T.storage), T.cbytes), 0, 0, 0));
   DRB_TRY(build_pipe_plan(T.pipe, T.m, cp.data(), sizeof(RI),
                           plan_group(dtype_bytes(T.storage), T.cbytes), 0, 0));
+  // A^T of a short-row matrix (a stencil) has short rows too: x-bar then
+  // runs on its sliced-ELL copy, as the forward product does
+  DRB_TRY(sell_build(T, cp.data(), sizeof(RI), s));
   return DRB_OK;
 }
 
@@ -334,7 +337,7 @@ drb_status adjoint_refresh_values(Csr &A, cudaStream_t s) {
   }
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
-  return DRB_OK;
+  return sell_pack_values(*A.tr, s);
 }
 
 drb_status spmv_t_launch(Csr &A, const void *ybar, void *xbar, cudaStream_t s) {

@@ -6,9 +6,9 @@
 // nonzeros (a 5-point stencil) that bookkeeping costs more than the bytes it
 // moves.  Here rows are grouped in slices of 32 consecutive rows; slice s is
 // padded to its longest row, w_s, and stored k-major: element k of row
-// 32*s + lane sits at off[s] + 32*k + lane.  One warp runs one slice with
-// lane = row, so every load of values and column indices is one coalesced
-// 128/256-byte line, and x gathers of a banded matrix (neighbouring rows,
+// 32*s + lane sits at off[s] + 32*k + lane.  A warp runs one slice (two for
+// f32) per step with lane = row, so every load of values and column indices
+// is one coalesced 128/256-byte line, and x gathers of a banded matrix (neighbouring rows,
 // neighbouring columns) coalesce too.  Each row is summed by its own lane in
 // k order, so results are deterministic.  Padding entries carry value 0 and
 // the row's last column (x stays in a cached line).
@@ -33,7 +33,6 @@ using warpk::AccOf;
 using warpk::WarpResid;
 constexpr int kSellNT = 256;
 constexpr int kSellWarps = kSellNT / 32;
-constexpr int kSellK = 8;          // row elements loaded per step
 constexpr int kSellMaxWidth = 64;  // longest row a SELL copy accepts
 constexpr double kSellMaxPad = 1.2; // padded elements / nnz
 
@@ -86,7 +85,7 @@ __global__ void sell_pack(int64_t m, int64_t nrows_padded, const RI *__restrict_
   }
 }
 
-template <class V, bool RESID>
+template <class V, bool RESID, int NS, int K>
 __global__ void __launch_bounds__(kSellNT)
     sell_spmv(const V *__restrict__ vals, const int *__restrict__ cols,
               const int64_t *__restrict__ off, int64_t s0, int64_t s1, int64_t m,
@@ -106,42 +105,64 @@ __global__ void __launch_bounds__(kSellNT)
   const uint64_t pol_x = ptx::policy_evict_last();
   const Acc *bvec = static_cast<const Acc *>(ra.b);
   double r2 = 0.0;
-  for (int64_t sl = a; sl < b; sl++) {
-    const int64_t o = __ldg(off + sl);
-    const int wd = (int)((__ldg(off + sl + 1) - o) >> 5);
-    const V *vp = vals + o + lane;
-    const int *cp = cols + o + lane;
-    Acc acc = 0;
-    for (int k0 = 0; k0 < wd; k0 += kSellK) {
-      V v[kSellK];
-      int c[kSellK];
+  for (int64_t sl = a; sl < b; sl += NS) {
+    int64_t o[NS];
+    int wd[NS];
+    int wmax = 0;
 #pragma unroll
-      for (int q = 0; q < kSellK; q++) {
-        v[q] = V(0);
-        c[q] = 0;
-        if (k0 + q < wd) {
-          v[q] = ld_stream(vp + 32 * (k0 + q), pol_s);
-          c[q] = ld_stream(cp + 32 * (k0 + q), pol_s);
-        }
+    for (int j = 0; j < NS; j++) {
+      wd[j] = 0;
+      o[j] = 0;
+      if (sl + j < b) {
+        o[j] = __ldg(off + sl + j);
+        wd[j] = (int)((__ldg(off + sl + j + 1) - o[j]) >> 5);
       }
-      Acc xv[kSellK];
-#pragma unroll
-      for (int q = 0; q < kSellK; q++)
-        xv[q] = k0 + q < wd ? warpk::ld_x(x + c[q], pol_x) : Acc(0);
-#pragma unroll
-      for (int q = 0; q < kSellK; q++)
-        if (k0 + q < wd)
-          acc += (Acc)v[q] * xv[q];
+      wmax = max(wmax, wd[j]);
     }
-    const int64_t row = sl * 32 + lane;
-    if (row < m) {
-      y[row] = acc;
-      if (RESID) {
-        if (ra.dot) {
-          r2 += (double)acc * (double)bvec[row];
-        } else {
-          const double dd = (double)acc - (double)bvec[row];
-          r2 += dd * dd;
+    Acc acc[NS];
+#pragma unroll
+    for (int j = 0; j < NS; j++)
+      acc[j] = 0;
+    for (int k0 = 0; k0 < wmax; k0 += K) {
+      V v[NS][K];
+      int c[NS][K];
+#pragma unroll
+      for (int j = 0; j < NS; j++)
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+          v[j][q] = V(0);
+          c[j][q] = 0;
+          if (k0 + q < wd[j]) {
+            const int64_t e = o[j] + 32 * (k0 + q) + lane;
+            v[j][q] = ld_stream(vals + e, pol_s);
+            c[j][q] = ld_stream(cols + e, pol_s);
+          }
+        }
+      Acc xv[NS][K];
+#pragma unroll
+      for (int j = 0; j < NS; j++)
+#pragma unroll
+        for (int q = 0; q < K; q++)
+          xv[j][q] = k0 + q < wd[j] ? warpk::ld_x(x + c[j][q], pol_x) : Acc(0);
+#pragma unroll
+      for (int j = 0; j < NS; j++)
+#pragma unroll
+        for (int q = 0; q < K; q++)
+          if (k0 + q < wd[j])
+            acc[j] += (Acc)v[j][q] * xv[j][q];
+    }
+#pragma unroll
+    for (int j = 0; j < NS; j++) {
+      const int64_t row = (sl + j) * 32 + lane;
+      if (sl + j < b && row < m) {
+        y[row] = acc[j];
+        if (RESID) {
+          if (ra.dot) {
+            r2 += (double)acc[j] * (double)bvec[row];
+          } else {
+            const double dd = (double)acc[j] - (double)bvec[row];
+            r2 += dd * dd;
+          }
         }
       }
     }
@@ -183,12 +204,12 @@ __global__ void __launch_bounds__(kSellNT)
   }
 }
 
-template <class V, bool RESID> int sell_grid(int dev) {
+template <class V, bool RESID, int NS, int K> int sell_grid(int dev) {
   static int cache[64] = {0};
   int &g = cache[dev < 64 ? dev : 0];
   if (g == 0) {
     int occ = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sell_spmv<V, RESID>, kSellNT, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sell_spmv<V, RESID, NS, K>, kSellNT, 0) !=
             cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
       return 148;
@@ -197,30 +218,45 @@ template <class V, bool RESID> int sell_grid(int dev) {
   return g;
 }
 
-template <class V>
-drb_status sell_typed(Csr &A, const void *x, void *y, const WarpResid *ra, int64_t s0,
-                      int64_t s1, cudaStream_t s) {
+template <class V, int NS, int K>
+drb_status sell_run(Csr &A, const void *x, void *y, const WarpResid *ra, int64_t s0,
+                    int64_t s1, cudaStream_t s) {
   using Acc = typename AccOf<V>::type;
   const Sell &S = A.sell;
-  if (s1 <= s0)
-    return DRB_OK;
-  const int64_t need = (s1 - s0 + kSellWarps - 1) / kSellWarps;
+  const int64_t need = (s1 - s0 + kSellWarps * NS - 1) / (kSellWarps * NS);
   WarpResid r{};
   if (ra) {
     r = *ra;
-    const int g = (int)std::min<int64_t>(sell_grid<V, true>(A.device), need);
-    sell_spmv<V, true><<<g, kSellNT, 0, s>>>(S.vals.as<V>(), S.cols.as<int>(),
-                                            S.off.as<int64_t>(), s0, s1, A.m,
-                                            static_cast<const V *>(x), static_cast<Acc *>(y), r);
+    const int g = (int)std::min<int64_t>(sell_grid<V, true, NS, K>(A.device), need);
+    sell_spmv<V, true, NS, K><<<g, kSellNT, 0, s>>>(S.vals.as<V>(), S.cols.as<int>(),
+                                                   S.off.as<int64_t>(), s0, s1, A.m,
+                                                   static_cast<const V *>(x),
+                                                   static_cast<Acc *>(y), r);
   } else {
-    const int g = (int)std::min<int64_t>(sell_grid<V, false>(A.device), need);
-    sell_spmv<V, false><<<g, kSellNT, 0, s>>>(S.vals.as<V>(), S.cols.as<int>(),
-                                             S.off.as<int64_t>(), s0, s1, A.m,
-                                             static_cast<const V *>(x), static_cast<Acc *>(y), r);
+    const int g = (int)std::min<int64_t>(sell_grid<V, false, NS, K>(A.device), need);
+    sell_spmv<V, false, NS, K><<<g, kSellNT, 0, s>>>(S.vals.as<V>(), S.cols.as<int>(),
+                                                    S.off.as<int64_t>(), s0, s1, A.m,
+                                                    static_cast<const V *>(x),
+                                                    static_cast<Acc *>(y), r);
   }
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
   return DRB_OK;
+}
+
+// Slices per warp step and row elements per load step, per element type:
+// measured on the 2048^2 Laplacian, f64 is best with one slice of 8 (56 us;
+// two slices 58-87 us: the extra registers cost occupancy), f32 with two
+// slices of 6 (39.5 us against 42 us for one of 8).
+template <class V>
+drb_status sell_typed(Csr &A, const void *x, void *y, const WarpResid *ra, int64_t s0,
+                      int64_t s1, cudaStream_t s) {
+  if (s1 <= s0)
+    return DRB_OK;
+  if constexpr (sizeof(V) == 4)
+    return sell_run<V, 2, 6>(A, x, y, ra, s0, s1, s);
+  else
+    return sell_run<V, 1, 8>(A, x, y, ra, s0, s1, s);
 }
 
 template <class V, class RI>

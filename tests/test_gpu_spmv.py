@@ -408,12 +408,22 @@ def test_residual_norm2(mp, dtype):
 
 # ---- adjoint ------------------------------------------------------------------------
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-def test_adjoint_against_transposed_oracle(mp, dtype):
-    rp, ci, v, m, n = chunky_matrix(dtype)
+@pytest.mark.parametrize("kind", ["chunky", "laplacian"])
+def test_adjoint_against_transposed_oracle(mp, dtype, kind):
+    """Row-block kernels (irregular rows), and the sliced-ELL copies of A and
+    A^T (a Laplacian with random values: short regular rows both ways)."""
+    if kind == "chunky":
+        rp, ci, v, m, n = chunky_matrix(dtype)
+    else:
+        import drb
+        rp, ci, v = drb.gen.laplacian2d_csr(300, value_dtype=dtype)
+        m = n = 300 * 300
+        v = np.random.default_rng(5).uniform(-1, 1, len(v)).astype(dtype)
     rng = np.random.default_rng(2)
     x = rng.uniform(-1, 1, n).astype(dtype)
     yb = rng.uniform(-1, 1, m).astype(dtype)
     a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0, adjoint=True)
+    assert (a.variant() == 2048) == (kind == "laplacian")
     tdt = torch.from_numpy(x).dtype
     xbar = torch.empty(n, dtype=tdt, device="cuda")
     abar = torch.empty(len(v), dtype=tdt, device="cuda")
