@@ -65,10 +65,36 @@ class _Comm:
 
 
 _COMM = _Comm()
+_DIST_COMM = None
 
 
-def default_comm() -> _Comm:
+def default_comm():
+    """Rank 0 of 1, or -- when torch.distributed is initialised with more
+    than one rank (one process per GPU) -- the world group as a
+    communicator (drb.dist.DistComm)."""
+    global _DIST_COMM
+    if torch.distributed.is_available() and torch.distributed.is_initialized() and \
+            torch.distributed.get_world_size() > 1:
+        if _DIST_COMM is None:
+            from .dist import DistComm
+            _DIST_COMM = DistComm()
+        return _DIST_COMM
     return _COMM
+
+
+class _DeviceBlock:
+    """A rank's segment as a single-process device handle on its GPU (the
+    local product of a multi-process matrix)."""
+
+    def __init__(self, rowptr, colind, values, shape, **kw):
+        self.a = distributed_sparse_matrix(csr_matrix_view(values, rowptr, colind, shape), 0,
+                                           distr=csr_row_distribution, comm=_COMM, **kw)
+        self.rows = shape[0]
+
+    def gemv(self, x: torch.Tensor, k: int) -> torch.Tensor:
+        y = torch.empty(self.rows * k, dtype=self.a.compute_dtype, device="cuda")
+        self.a.gemv_device(x.to(device="cuda", dtype=self.a.x_dtype), y, k, capi.DRB_COL_MAJOR)
+        return y
 
 
 def init(device: int | None = None) -> None:
@@ -165,14 +191,15 @@ class _Segment:
     """One row-block segment (the reference's csr_row_segment /
     csr_eq_segment): rank(), size(), is_local(), iteration over entries."""
 
-    def __init__(self, mat: "distributed_sparse_matrix", idx: int):
+    def __init__(self, mat: "distributed_sparse_matrix", idx: int, bounds=None):
         self._m = mat
         self._idx = idx
-        r0, r1, z0, z1 = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64())
-        check(capi.lib.drb_csr_segment(mat._h, idx, C.byref(r0), C.byref(r1),
-                                       C.byref(z0), C.byref(z1)))
-        self.row_begin, self.row_end = r0.value, r1.value
-        self.nnz_begin, self.nnz_end = z0.value, z1.value
+        if bounds is None:
+            r0, r1, z0, z1 = (C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64())
+            check(capi.lib.drb_csr_segment(mat._h, idx, C.byref(r0), C.byref(r1),
+                                           C.byref(z0), C.byref(z1)))
+            bounds = (r0.value, r1.value, z0.value, z1.value)
+        self.row_begin, self.row_end, self.nnz_begin, self.nnz_end = bounds
 
     def rank(self) -> int:
         return self._idx
@@ -184,7 +211,9 @@ class _Segment:
         return self.size()
 
     def is_local(self) -> bool:
-        return True  # every segment lives on this process's GPU
+        sh = self._m._sharded
+        # one process: every segment lives on its GPU; several: rank r's
+        return sh is None or sh.comm.rank() == self._idx
 
     def entries(self):
         return self._m._entries(self.nnz_begin, self.size())
@@ -213,11 +242,30 @@ class distributed_sparse_matrix:
                  *, distr=csr_eq_distribution, nsegments: int = 1,
                  storage=None, adjoint: bool = False,
                  keep_index64: bool = False, autotune: bool = False,
-                 compensated: bool = False, x_dtype=None, stream=None):
+                 compensated: bool = False, x_dtype=None, stream=None,
+                 comm=None, local_block=None):
+        self._h = C.c_void_p(0)
+        self._sharded = None
+        self.distribution = dist or distribution()
+        comm = comm if comm is not None else default_comm()
+        if comm.size() > 1:
+            # one segment per rank (drb.dist): this rank's rows on its GPU
+            from .dist import ShardedCsr
+            opts = dict(adjoint=adjoint, keep_index64=keep_index64, autotune=autotune,
+                        compensated=compensated)
+            factory = local_block or (lambda rp, ci, v, shape: _DeviceBlock(rp, ci, v, shape,
+                                                                            **opts))
+            self._sharded = ShardedCsr(csr_view, root, distr.partition == capi.DRB_PART_EQ,
+                                       comm, factory)
+            sh = self._sharded
+            self._shape = (sh.m, sh.n)
+            self._nnz = sh.nnz
+            self.value_dtype = self.storage_dtype = self.compute_dtype = sh.dtype
+            self.x_dtype = sh.dtype
+            self._ybuf = {}
+            return
         if root != 0:
             raise ValueError(f"root {root} is not a rank: one process owns the GPU")
-        self._h = C.c_void_p(0)
-        self.distribution = dist or distribution()
         values = np.ascontiguousarray(csr_view.values_data())
         rowptr = np.ascontiguousarray(csr_view.rowptr_data())
         colind = np.ascontiguousarray(csr_view.colind_data())
@@ -272,12 +320,21 @@ class distributed_sparse_matrix:
         return self._nnz
 
     def segments(self) -> list:
+        if self._sharded is not None:
+            return [_Segment(self, r, tuple(b)) for r, *b in self._sharded.segments()]
         nseg = C.c_int()
         check(capi.lib.drb_csr_num_segments(self._h, C.byref(nseg)))
         return [_Segment(self, i) for i in range(nseg.value)]
 
     def fence(self) -> None:
+        if self._sharded is not None:
+            torch.distributed.barrier(group=self._sharded.comm.group)
+            return
         torch.cuda.current_stream().synchronize()
+
+    def local(self):
+        """This rank's segment as a local block (several ranks), else self."""
+        return self._sharded.local if self._sharded is not None else self
 
     def storage_bytes(self):
         v, c, r = C.c_int(), C.c_int(), C.c_int()
@@ -285,6 +342,12 @@ class distributed_sparse_matrix:
         return v.value, c.value, r.value
 
     def _entries(self, offset: int, count: int):
+        if self._sharded is not None:
+            if not hasattr(self, "_all"):
+                self._all = self._sharded.all_entries()
+            r, c, v = self._all
+            return (r[offset:offset + count], c[offset:offset + count],
+                    v[offset:offset + count].astype(np.float64))
         rows = np.empty(count, np.int64)
         cols = np.empty(count, np.int64)
         vals = np.empty(count, np.float64)
@@ -303,13 +366,20 @@ class distributed_sparse_matrix:
 
     @property
     def handle(self) -> C.c_void_p:
+        if self._sharded is not None:
+            blk = self._sharded.local
+            return blk.a.handle if isinstance(blk, _DeviceBlock) else C.c_void_p(0)
         return self._h
 
     # ---- the hot call ----
     def local_gemv_and_collect(self, root: int, res, x: torch.Tensor,
                                width: int, stream=None) -> None:
         """distributed_sparse_matrix.hpp:153-158: y = A x for `width` RHS
-        (column-major), result written into `res` on root."""
+        (column-major), result written into `res` on root (on every rank
+        when root is None)."""
+        if self._sharded is not None:
+            self._sharded.gemv(root, res, x, width)
+            return
         m = self._shape[0]
         if isinstance(res, torch.Tensor) and res.is_cuda:
             y = res
@@ -387,6 +457,11 @@ class broadcasted_vector:
 
     def broadcast_data(self, data_size: int, root: int, root_data,
                        comm=None, dtype=None) -> None:
+        comm = comm if comm is not None else default_comm()
+        if comm.size() > 1:
+            from .dist import broadcast_tensor
+            self._data = broadcast_tensor(comm, root, root_data, data_size, dtype)
+            return
         if root != 0:
             raise ValueError(f"root {root} is not a rank")
         t = torch.as_tensor(np.asarray(root_data) if not isinstance(root_data, torch.Tensor) else root_data)
@@ -410,6 +485,15 @@ class broadcasted_vector:
         return self._data[i]
 
 
+def _slim_array(root_data, height: int, width: int) -> np.ndarray:
+    """The T** overload (a list of `width` columns) or one flat
+    column-major block, as a flat array of height*width elements."""
+    if isinstance(root_data, (list, tuple)) and root_data and hasattr(root_data[0], "__len__") \
+            and len(root_data) == width and not isinstance(root_data[0], (int, float)):
+        return np.concatenate([np.asarray(c)[:height] for c in root_data])
+    return np.asarray(root_data).reshape(-1)[: height * width]
+
+
 class broadcasted_slim_matrix:
     """A height x width block replicated on every rank, column-major:
     element (i, j) at i + j*height (broadcasted_slim_matrix.hpp:9-80)."""
@@ -421,6 +505,15 @@ class broadcasted_slim_matrix:
 
     def broadcast_data(self, height: int, width: int, root: int, root_data,
                        comm=None, dtype=None) -> None:
+        comm = comm if comm is not None else default_comm()
+        if comm.size() > 1:
+            from .dist import broadcast_tensor
+            arr = None
+            if comm.rank() == root:
+                arr = _slim_array(root_data, height, width)
+            self._data = broadcast_tensor(comm, root, arr, height * width, dtype)
+            self._width, self._height = width, height
+            return
         if root != 0:
             raise ValueError(f"root {root} is not a rank")
         if isinstance(root_data, (list, tuple)) and root_data and hasattr(root_data[0], "__len__") \
@@ -459,19 +552,26 @@ def gemv(*args, stream=None) -> None:
         root, res, a, b = args
     elif len(args) == 3:
         res, a, b = args
-        root = 0
+        root = None
     else:
         raise TypeError("gemv(root, res, A, b) or gemv(res, A, b)")
-    if root != default_comm().rank():
-        raise ValueError(f"root {root} is not a rank: one process owns the GPU")
+    sharded = getattr(a, "_sharded", None) is not None
+    if not sharded:
+        if root is None:
+            root = 0  # one rank: the root's result is everyone's
+        if root != default_comm().rank():
+            raise ValueError(f"root {root} is not a rank: one process owns the GPU")
+    elif root is not None and not 0 <= root < a._sharded.comm.size():
+        raise ValueError(f"root {root} is not a rank")
     m, n = a.shape()
+    on_root = root is None or not sharded or a._sharded.comm.rank() == root
     if isinstance(b, broadcasted_slim_matrix):
         width = b.width()
-        if m * width != len(res):
+        if on_root and m * width != len(res):
             raise ValueError(f"res has {len(res)} elements, expected {m * width}")
     else:
         width = 1
-        if m != len(res):
+        if on_root and m != len(res):
             raise ValueError(f"res has {len(res)} elements, expected {m}")
         if b.size() != n:
             raise ValueError(f"x has {b.size()} elements, expected {n}")
