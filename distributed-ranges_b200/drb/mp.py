@@ -412,7 +412,8 @@ class distributed_sparse_matrix:
                                          int(k), layout, _stream(stream)))
 
     def variant(self) -> int:
-        """Single-RHS kernel variant: item span (256/512) | 1 if skewed."""
+        """Single-RHS kernel variant: item span (256/512) | 1 if skewed, or
+        2048 for the sliced-ELL copy (short, regular rows)."""
         v = C.c_int()
         check(capi.lib.drb_csr_variant(self._h, C.byref(v)))
         return v.value

@@ -156,7 +156,12 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
 
 /* Kernel variant of the single right-hand-side product: item span (256 or
  * 512 nonzeros) | 1 when the skewed (bank-conflict-free) product layout is
- * used.  drb_csr_autotune times the four variants on this matrix's sparsity
+ * used, or 2048 for the sliced-ELL copy (slices of 32 rows padded to their
+ * longest row, lane = row), which drb_csr_create takes by default when the
+ * longest row has <= 64 nonzeros, padding adds <= 20% and twice the copy's
+ * size is free (the copy costs padded * (value + 4) bytes; the CSR arrays
+ * stay for the other paths).  drb_csr_autotune times the row-block variants
+ * and, when the matrix qualifies, the sliced copy on this matrix's sparsity
  * pattern, keeps the fastest (also for the adjoint's transposed matrix) and
  * returns it; it synchronises `stream`.  Results are identical across
  * variants up to the summation order inside a row. */
