@@ -902,7 +902,9 @@ def profile_case(name):
       dense_f32  the single-matrix dense gemv at 16384 x 16384 FP32 (1 GB,
                above L2), one right-hand side;
       laplacian_f64  the single-RHS SpMV on the 2048^2 5-point Laplacian
-               (4,194,304 rows, FP64 values, int32 indices; 335 MB)."""
+               (4,194,304 rows, FP64 values, int32 indices; 335 MB);
+      cg_f64   conjugate gradients on that Laplacian, FP64: one warm-up solve
+               of 8 iterations, then 24 iterations (rtol 0)."""
     import torch
     import drb
     from drb import mp
@@ -960,6 +962,17 @@ def profile_case(name):
         for _ in range(4):
             A.gemv_device(x, y)
         A.check()
+    elif name == "cg_f64":
+        rp, ci, v = drb.gen.laplacian2d_csr(2048, value_dtype=np.float64)
+        m = len(rp) - 1
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp.astype(np.int32), ci, (m, m)),
+                                         0, distr=mp.csr_row_distribution)
+        g = torch.Generator(device="cuda").manual_seed(SEED + 11)
+        b = torch.randn(m, device="cuda", dtype=torch.float64, generator=g)
+        x = torch.zeros(m, device="cuda", dtype=torch.float64)
+        mp.conjugate_gradient(A, b, x, max_iters=8, rtol=0.0)
+        x.zero_()
+        mp.conjugate_gradient(A, b, x, max_iters=24, rtol=0.0)
     else:
         raise SystemExit(f"unknown profile case {name}")
     print("profile case", name, "done", flush=True)
@@ -980,7 +993,7 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
-    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64"],
+    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64", "cg_f64"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
