@@ -28,7 +28,10 @@ namespace drb {
 
 namespace {
 constexpr int kCgNT = 256;
-constexpr int kCgGrid = 592; // 4 CTAs per SM; fixed, so sums are deterministic
+// 3 CTAs per SM, all resident at once (the kernels are bounded to fit);
+// fixed, so the sums are deterministic
+constexpr int kCgGrid = 148 * 3;
+constexpr int kCgMinBlocks = 3;
 constexpr int kCgBlock = 8;  // iterations per graph replay
 
 enum : int { kRunning = 0, kConverged = 1, kBreakdown = 2, kMaxIters = 3 };
@@ -134,7 +137,7 @@ __device__ bool grid_sums(const double (&v)[NV], double *partials, int *ticket,
 // r = b - q (q = A x0), p = r; rr = r.r, bb = b.b; the stop word starts the
 // loop (or ends it at once when x0 already meets the tolerance).
 template <class T>
-__global__ void __launch_bounds__(kCgNT)
+__global__ void __launch_bounds__(kCgNT, kCgMinBlocks)
     cg_init(int64_t n, const T *__restrict__ b, const T *__restrict__ q, T *__restrict__ r,
             T *__restrict__ p, CgState *st, double rtol, int64_t max_iters,
             double *partials, int *ticket) {
@@ -161,9 +164,18 @@ __global__ void __launch_bounds__(kCgNT)
   }
 }
 
+// 16 bytes of T (two doubles or four floats).
+template <class T> union Vec16T {
+  uint4 u;
+  T t[16 / sizeof(T)];
+};
+
 // alpha = rr / p.q; x += alpha p; r -= alpha q; rr' = r.r; beta = rr' / rr.
-template <class T>
-__global__ void __launch_bounds__(kCgNT)
+// With VEC (x, r, p, q all 16-byte aligned) every thread moves 16-byte
+// vectors, two of them per loop trip, so enough bytes are in flight to
+// stream at the HBM rate; the scalar tail follows.
+template <class T, bool VEC>
+__global__ void __launch_bounds__(kCgNT, kCgMinBlocks)
     cg_update(int64_t n, T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
               const T *__restrict__ q, CgState *st, double *partials, int *ticket) {
   const volatile CgState *vs = st;
@@ -178,8 +190,43 @@ __global__ void __launch_bounds__(kCgNT)
     return;
   }
   double acc[1] = {0.0};
+  const int64_t tid = (int64_t)blockIdx.x * kCgNT + threadIdx.x;
   const int64_t nth = (int64_t)gridDim.x * kCgNT;
-  for (int64_t i = (int64_t)blockIdx.x * kCgNT + threadIdx.x; i < n; i += nth) {
+  int64_t done = 0;
+  if (VEC) {
+    constexpr int PER = 16 / sizeof(T);
+    const int64_t nv = n / PER;
+    auto step = [&](int64_t i, Vec16T<T> &vx, Vec16T<T> &vr, const Vec16T<T> &vp,
+                    const Vec16T<T> &vq) {
+#pragma unroll
+      for (int e = 0; e < PER; e++) {
+        vx.t[e] = (T)((double)vx.t[e] + alpha * (double)vp.t[e]);
+        vr.t[e] = (T)((double)vr.t[e] - alpha * (double)vq.t[e]);
+        acc[0] += (double)vr.t[e] * (double)vr.t[e];
+      }
+      reinterpret_cast<uint4 *>(x)[i] = vx.u;
+      reinterpret_cast<uint4 *>(r)[i] = vr.u;
+    };
+    for (int64_t i = tid; i < nv; i += 2 * nth) {
+      const int64_t j = i + nth;
+      Vec16T<T> x0, r0, p0, q0, x1, r1, p1, q1;
+      x0.u = reinterpret_cast<const uint4 *>(x)[i];
+      r0.u = reinterpret_cast<const uint4 *>(r)[i];
+      p0.u = __ldg(reinterpret_cast<const uint4 *>(p) + i);
+      q0.u = __ldg(reinterpret_cast<const uint4 *>(q) + i);
+      if (j < nv) {
+        x1.u = reinterpret_cast<const uint4 *>(x)[j];
+        r1.u = reinterpret_cast<const uint4 *>(r)[j];
+        p1.u = __ldg(reinterpret_cast<const uint4 *>(p) + j);
+        q1.u = __ldg(reinterpret_cast<const uint4 *>(q) + j);
+      }
+      step(i, x0, r0, p0, q0);
+      if (j < nv)
+        step(j, x1, r1, p1, q1);
+    }
+    done = nv * PER;
+  }
+  for (int64_t i = done + tid; i < n; i += nth) {
     const T xi = (T)((double)x[i] + alpha * (double)p[i]);
     const T ri = (T)((double)r[i] - alpha * (double)q[i]);
     x[i] = xi;
@@ -197,16 +244,39 @@ __global__ void __launch_bounds__(kCgNT)
   }
 }
 
-// p = r + beta p.
+// p = r + beta p (r and p are the plan's own, 16-byte aligned buffers).
 template <class T>
-__global__ void __launch_bounds__(kCgNT)
+__global__ void __launch_bounds__(kCgNT, kCgMinBlocks)
     cg_pupdate(int64_t n, const T *__restrict__ r, T *__restrict__ p, const CgState *st) {
   const volatile CgState *vs = st;
   if (vs->done != kRunning)
     return;
   const double beta = vs->beta;
+  constexpr int PER = 16 / sizeof(T);
+  const int64_t tid = (int64_t)blockIdx.x * kCgNT + threadIdx.x;
   const int64_t nth = (int64_t)gridDim.x * kCgNT;
-  for (int64_t i = (int64_t)blockIdx.x * kCgNT + threadIdx.x; i < n; i += nth)
+  const int64_t nv = n / PER;
+  for (int64_t i = tid; i < nv; i += 2 * nth) {
+    const int64_t j = i + nth;
+    Vec16T<T> r0, p0, r1, p1;
+    r0.u = __ldg(reinterpret_cast<const uint4 *>(r) + i);
+    p0.u = reinterpret_cast<const uint4 *>(p)[i];
+    if (j < nv) {
+      r1.u = __ldg(reinterpret_cast<const uint4 *>(r) + j);
+      p1.u = reinterpret_cast<const uint4 *>(p)[j];
+    }
+#pragma unroll
+    for (int e = 0; e < PER; e++)
+      p0.t[e] = (T)((double)r0.t[e] + beta * (double)p0.t[e]);
+    reinterpret_cast<uint4 *>(p)[i] = p0.u;
+    if (j < nv) {
+#pragma unroll
+      for (int e = 0; e < PER; e++)
+        p1.t[e] = (T)((double)r1.t[e] + beta * (double)p1.t[e]);
+      reinterpret_cast<uint4 *>(p)[j] = p1.u;
+    }
+  }
+  for (int64_t i = nv * PER + tid; i < n; i += nth)
     p[i] = (T)((double)r[i] + beta * (double)p[i]);
 }
 
@@ -221,10 +291,17 @@ drb_status enqueue_iterations(Csr &A, CgPlan &C, T *x, int iters, cudaStream_t s
   auto *st = C.state.as<CgState>();
   double *partials = C.scratch.as<double>();
   int *ticket = reinterpret_cast<int *>(partials + 2 * kCgGrid);
+  // x is the caller's buffer: the 16-byte path needs it aligned (r, p and q
+  // are the plan's own allocations)
+  const bool vec = reinterpret_cast<uintptr_t>(x) % 16 == 0;
   for (int k = 0; k < iters; k++) {
     DRB_TRY(rowdot_pipe_launch(A, C.p.p, C.p.p, C.q.p, &st->pq, &st->done, s));
-    cg_update<T><<<grid, kCgNT, 0, s>>>(n, x, C.r.as<T>(), C.p.as<T>(), C.q.as<T>(), st,
-                                        partials, ticket);
+    if (vec)
+      cg_update<T, true><<<grid, kCgNT, 0, s>>>(n, x, C.r.as<T>(), C.p.as<T>(), C.q.as<T>(),
+                                                st, partials, ticket);
+    else
+      cg_update<T, false><<<grid, kCgNT, 0, s>>>(n, x, C.r.as<T>(), C.p.as<T>(), C.q.as<T>(),
+                                                 st, partials, ticket);
     cg_pupdate<T><<<grid, kCgNT, 0, s>>>(n, C.r.as<T>(), C.p.as<T>(), st);
     note_launch(2);
     DRB_CUDA_TRY(cudaGetLastError());
