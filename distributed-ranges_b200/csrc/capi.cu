@@ -547,6 +547,16 @@ drb_status build_row_segments(Csr &A, int target) {
   }
   P.seg_i0.push_back((int64_t)it.size());
   P.seg_r0.push_back(A.m);
+  // chunks are numbered in row order and a split row stays in one segment,
+  // so segment g's chunks are the contiguous range [seg_c0[g], seg_c0[g+1])
+  P.seg_c0.assign(1, 0);
+  for (size_t g = 0; g + 1 < P.seg_i0.size(); g++) {
+    int64_t cend = P.seg_c0.back();
+    for (int64_t i = P.seg_i0[g]; i < P.seg_i0[g + 1]; i++)
+      if (it[(size_t)i].nrows == 0)
+        cend = std::max<int64_t>(cend, (int64_t)it[(size_t)i].chunk + 1);
+    P.seg_c0.push_back(cend);
+  }
   DRB_TRY(P.seg_items.alloc(sizeof(Item) * std::max<size_t>(it.size(), 1)));
   DRB_CUDA_TRY(cudaMemcpy(P.seg_items.p, it.data(), sizeof(Item) * it.size(),
                           cudaMemcpyHostToDevice));
@@ -614,9 +624,13 @@ drb_status gemv_host_segmented(Csr &A, const void *x_host, void *y_host,
     } else {
       P.items.p = P.seg_items.as<Item>() + P.seg_i0[g];
       P.nitems = P.seg_i0[g + 1] - P.seg_i0[g];
+      P.fin_c0 = P.seg_c0[g];
+      P.fin_c1 = P.seg_c0[g + 1];
       st = spmv_pipe_launch(A, A.xh_dev.p, A.yh_dev.p, s);
       P.items.p = items0;
       P.nitems = n0;
+      P.fin_c0 = 0;
+      P.fin_c1 = -1;
     }
     if (st == DRB_OK && cudaEventRecord(A.seg_done[g], s) != cudaSuccess)
       st = DRB_ERR_CUDA;

@@ -141,7 +141,7 @@ struct PipePlan {
   DevBuf items;    // Item[nitems]
   DevBuf chunks;   // Chunk[nchunks]
   DevBuf partials; // value type [nchunks]
-  DevBuf counters; // int[nsplit]
+  DevBuf counters; // unsigned work counter of the persistent kernel (zeroed per launch)
   DevBuf err;      // int: device-side error word (DRB_ERR_TIMEOUT)
   DevBuf red;      // double[grid] + int ticket: fused residual
   // The same items ordered by row and cut into row segments (built on the
@@ -149,6 +149,8 @@ struct PipePlan {
   // and covers rows [seg_r0[s], seg_r0[s+1]).
   DevBuf seg_items;
   std::vector<int64_t> seg_i0, seg_r0;
+  std::vector<int64_t> seg_c0;      // first chunk of each segment (+ end)
+  int64_t fin_c0 = 0, fin_c1 = -1;  // chunks the plain launch finishes (-1: all)
   uint64_t gen = 0; // bumped by every (re)build
 };
 

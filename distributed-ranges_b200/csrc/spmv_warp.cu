@@ -18,13 +18,14 @@ using warpk::WarpResid;
 // argument (0 = choose).  The choice does not change results beyond the
 // summation order of a chunked row, which is the same for both layouts.
 //
-// Heuristic (measured on B200): rows shorter than a warp of lanes per row
-// favour 256-nonzero items with the skewed layout (bank-conflict-free row
-// sums); matrices whose nonzeros sit mostly in long rows favour 512-nonzero
-// items (fewer chunks) with vector product stores.  The environment variable
-// DRB_SPMV_VARIANT="tile,skew" (e.g. "512,0") overrides the heuristic for
-// handles created afterwards; drb_csr_autotune measures all four instead.
-int choose_pipe_variant(int64_t m, const void *rowptr_host, int rbytes) {
+// Default (measured on B200, random columns, 336M nonzeros, 64 MB x):
+// 256-nonzero items with the skewed layout are fastest or tied at every row
+// length (fixed rows of 16..4096 nonzeros: 1.33-1.49 ms; the bench's
+// power-law: 1.61 ms against 1.97 ms for 512-nonzero items) once chunked
+// rows finish in a separate pass.  The environment variable
+// DRB_SPMV_VARIANT="tile,skew" (e.g. "512,0") overrides it for handles
+// created afterwards; drb_csr_autotune measures all four instead.
+int choose_pipe_variant(int64_t, const void *, int) {
   if (const char *e = std::getenv("DRB_SPMV_VARIANT")) {
     const int t = std::atoi(e);
     const char *c = std::strchr(e, ',');
@@ -32,20 +33,7 @@ int choose_pipe_variant(int64_t m, const void *rowptr_host, int rbytes) {
     if (t == 256 || t == 512)
       return t | (sk ? 1 : 0);
   }
-  auto RP = [&](int64_t i) -> int64_t {
-    return rbytes == 4 ? (int64_t)((const int32_t *)rowptr_host)[i]
-                       : ((const int64_t *)rowptr_host)[i];
-  };
-  const int64_t nnz = m > 0 ? RP(m) : 0;
-  if (nnz == 0)
-    return 256 | 1;
-  int64_t in_long = 0;
-  for (int64_t r = 0; r < m; r++) {
-    const int64_t len = RP(r + 1) - RP(r);
-    if (len > 256)
-      in_long += len;
-  }
-  return (double)in_long / (double)nnz > 0.3 ? 512 : (256 | 1);
+  return 256 | 1;
 }
 
 drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
@@ -128,6 +116,7 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
     }
   }
   plan.seg_items.release(); // the row-segment order is rebuilt on demand
+  plan.seg_c0.clear();
   plan.seg_i0.clear();
   plan.seg_r0.clear();
   plan.nitems = (int64_t)all.size();
@@ -243,33 +232,57 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
     DRB_TRY(sell_build(A, rp.data(), A.rbytes, s));
   const int variants[5] = {256 | 1, 256, 512 | 1, 512, kVariantSell};
   const int nvar = A.sell.built ? 5 : 4;
+  float vms[5] = {3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f};
+  drb_status st = DRB_OK;
+  // Two rounds over the variants, each variant's best kept, after ~30 ms of
+  // warm-up launches: a first variant timed while the clocks still ramp up
+  // from idle would otherwise lose to a slower one timed later.
+  A.sell.on = false;
+  st = build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, variants[0], 0);
+  float warm = 0.f;
+  for (int w = 0; w < 50 && st == DRB_OK; w++) {
+    cudaEventRecord(e0, s);
+    st = spmv_pipe_launch(A, xb.p, yb.p, s);
+    cudaEventRecord(e1, s);
+    float ms = 0.f;
+    if (st != DRB_OK || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      break;
+    warm += ms;
+    if (w >= 4 && warm >= 30.f)
+      break;
+  }
+  for (int round = 0; round < 2 && st == DRB_OK; round++) {
+    for (int iv = 0; iv < nvar; iv++) {
+      const int v = variants[iv];
+      A.sell.on = v == kVariantSell;
+      if (!A.sell.on)
+        st = build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, v, 0);
+      if (st != DRB_OK)
+        break;
+      if ((st = spmv_pipe_launch(A, xb.p, yb.p, s)) != DRB_OK)
+        break;
+      cudaEventRecord(e0, s);
+      for (int i = 0; i < 3 && st == DRB_OK; i++)
+        st = spmv_pipe_launch(A, xb.p, yb.p, s);
+      cudaEventRecord(e1, s);
+      if (st != DRB_OK || cudaEventSynchronize(e1) != cudaSuccess)
+        break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      vms[iv] = std::min(vms[iv], ms);
+    }
+  }
   int best = variants[0], best_rb = variants[0];
   float best_ms = 3.4e38f, best_rb_ms = 3.4e38f;
-  drb_status st = DRB_OK;
   for (int iv = 0; iv < nvar; iv++) {
-    const int v = variants[iv];
-    A.sell.on = v == kVariantSell;
-    if (!A.sell.on)
-      st = build_pipe_plan(A.pipe, A.m, rp.data(), A.rbytes, group, v, 0);
-    if (st != DRB_OK)
-      break;
-    if ((st = spmv_pipe_launch(A, xb.p, yb.p, s)) != DRB_OK)
-      break;
-    cudaEventRecord(e0, s);
-    for (int i = 0; i < 3 && st == DRB_OK; i++)
-      st = spmv_pipe_launch(A, xb.p, yb.p, s);
-    cudaEventRecord(e1, s);
-    if (st != DRB_OK || cudaEventSynchronize(e1) != cudaSuccess)
-      break;
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = v;
+    if (vms[iv] < best_ms) {
+      best_ms = vms[iv];
+      best = variants[iv];
     }
-    if (v != kVariantSell && ms < best_rb_ms) {
-      best_rb_ms = ms;
-      best_rb = v;
+    if (variants[iv] != kVariantSell && vms[iv] < best_rb_ms) {
+      best_rb_ms = vms[iv];
+      best_rb = variants[iv];
     }
   }
   cudaEventDestroy(e0);

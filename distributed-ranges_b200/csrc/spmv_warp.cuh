@@ -2,9 +2,10 @@
 //
 // The matrix is cut once (build_pipe_plan, spmv_warp.cu) into work items of at
 // most TILE nonzeros counted from a 16-byte aligned start: up to kRows whole
-// short rows, or one fixed-size chunk of a long row.  Every warp of the grid
-// owns the items w, w + W, w + 2W, ... (W = warps in the grid) and runs them
-// with no CTA-wide barrier, so warps progress independently.
+// short rows, or one fixed-size chunk of a long row.  Warps take items in
+// batches of consecutive indices from a work counter (a fused row reduction:
+// items w, w + W, ..., W = warps in the grid) and run them with no CTA-wide
+// barrier, so warps progress independently.
 //
 // For its current item every lane holds TILE/32 nonzeros in registers
 // (16-byte vector loads of colind and values, evict-first L2 policy), gathers
@@ -26,9 +27,13 @@
 // rate (about one request per SM per clock); the design keeps many gathers in
 // flight per warp and as many warps as registers allow.
 //
-// A chunked long row writes one partial per chunk; the warp that completes
-// the last chunk (ticket counter) adds the partials in chunk order.  Every sum
-// has a fixed order, so results are deterministic.
+// A chunked long row writes one partial per chunk; a second small pass
+// (chunk_finish, or resid_finish with a fused row reduction) adds each split
+// row's partials in chunk order after the main launch.  (Finishing them in
+// the main launch -- the warp that completed a row's last chunk, found by an
+// atomic ticket -- made every chunk item wait on the ticket's round trip,
+// which cost a quarter of the time on long-row matrices.)  Every sum has a
+// fixed order, so results are deterministic.
 #pragma once
 
 #include <algorithm>
@@ -129,11 +134,11 @@ __device__ __forceinline__ int skew(int q) { return q + (q >> 5); }
 
 // Fused row reduction: ||A x - b||^2, or with `dot` set sum_i y_i b_i (b is
 // then a weight vector, e.g. p for p.Ap).  Whole rows add into a per-CTA
-// partial; a chunked row's term goes to its own slot because which warp
-// finishes it varies run to run.  The last CTA sums partials[0..grid) then
+// partial; a chunked row's term goes to its own slot rowres[counter],
+// written by the finish pass, whose last CTA sums partials[0..grid) then
 // rowres[0..nsplit) in order.  A non-null `stop` pointing at a non-zero word
-// makes the whole launch return before touching anything (a converged
-// iterative loop replaying a captured graph).
+// makes the launches return before touching anything (a converged iterative
+// loop replaying a captured graph).
 struct WarpResid {
   const void *b = nullptr;
   double *partials = nullptr;
@@ -326,33 +331,12 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     __syncwarp(); // the shared slice is rewritten by the next item
   }
 
-  // Lane 0 after a chunk: publish the partial; the last chunk of the row
-  // adds all partials in chunk order and writes y.
+  // Lane 0 after a chunk: publish the partial.  The split row is completed
+  // by a second pass (chunk_finish / resid_finish) in chunk order.
   template <bool RESID>
-  __device__ __forceinline__ void finish_chunk(const Item &cur, Acc tot, const Acc *bvec,
-                                               double *rowres, bool dotw) {
-    const Chunk ch = chunks[cur.chunk];
+  __device__ __forceinline__ void finish_chunk(const Item &cur, Acc tot, const Acc *,
+                                               double *, bool) {
     partials[cur.chunk] = tot;
-    __threadfence();
-    const int t = atomicAdd(&counters[ch.counter], 1);
-    if (t == ch.count - 1) {
-      __threadfence();
-      CSum<Acc> sum;
-      for (int i = 0; i < ch.count; i++) {
-        const Acc p = *(volatile Acc *)&partials[ch.first + i];
-        if (COMP)
-          sum.add(p);
-        else
-          sum.s += p;
-      }
-      const Acc v = sum.value();
-      y[ch.row] = v;
-      counters[ch.counter] = 0; // re-armed for the next launch
-      if (RESID) {
-        const double dd = (double)v - (double)bvec[ch.row];
-        rowres[ch.counter] = dotw ? (double)v * (double)bvec[ch.row] : dd * dd;
-      }
-    }
   }
 };
 
@@ -367,7 +351,6 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
   __shared__ int s_rp[kWarps][kRows + 1];
   __shared__ double s_red[kWarps];
-  __shared__ int s_last;
 
   if (RESID && ra.stop && *static_cast<const volatile int *>(ra.stop))
     return; // uniform: every CTA reads the same word, written by an earlier launch
@@ -376,21 +359,58 @@ __global__ void __launch_bounds__(kThreads)
                                       chunks, partials, counters,
                                       ptx::policy_evict_first(), ptx::policy_evict_last(),
                                       lane};
-  const int64_t nw = (int64_t)gridDim.x * kWarps;
-  int64_t it = (int64_t)blockIdx.x * kWarps + warp;
   const Acc *bvec = static_cast<const Acc *>(ra.b);
   double r2 = 0.0;
   Acc *prod = s_prod[warp];
   int *srp = s_rp[warp];
 
-  Slot<V, CI, TILE> A;
-  K.fetch(A, it);
-  while (A.valid) {
-    K.template process<RESID>(A, it + nw, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
-    it += nw;
+  // The plain product takes items in batches of kBatch consecutive indices
+  // from a work counter (zeroed before the launch; lane 0 takes the next
+  // index one item ahead, so the atomic's round trip overlaps the current
+  // item): a fixed round-robin share was sensitive to the exact sequence of
+  // item costs (the bench's power-law ran 2.23 ms against 1.61 ms for the
+  // same distribution with another seed; batched grabs: 1.53 ms for both).
+  // Which warp runs an item does not change any row's sum.  A fused row
+  // reduction adds rows into per-CTA partials, whose grouping would then
+  // vary run to run, so it keeps the fixed share (warp w: items w, w + W,
+  // ...) and stays deterministic.
+  if (RESID) {
+    const int64_t nw = (int64_t)gridDim.x * kWarps;
+    int64_t it = (int64_t)blockIdx.x * kWarps + warp;
+    Slot<V, CI, TILE> A;
+    K.fetch(A, it);
+    while (A.valid) {
+      K.template process<RESID>(A, it + nw, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
+      it += nw;
+    }
+  } else {
+    constexpr int kBatch = 8; // items per grab
+    auto grab = [&]() -> int64_t {
+      unsigned v = 0;
+      if (lane == 0)
+        v = atomicAdd(reinterpret_cast<unsigned *>(counters), (unsigned)kBatch);
+      return (int64_t)__shfl_sync(0xffffffffu, v, 0);
+    };
+    int64_t base = grab();
+    int k = 0;
+    auto advance = [&]() -> int64_t {
+      if (++k == kBatch) {
+        base = grab();
+        k = 0;
+      }
+      return base + k;
+    };
+    Slot<V, CI, TILE> A;
+    K.fetch(A, base);
+    int64_t next = advance();
+    while (A.valid) {
+      K.template process<RESID>(A, next, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
+      next = advance();
+    }
   }
 
   if (RESID) {
+    // the CTA's partial; resid_finish adds the split rows and combines
     const double t = wsum(r2);
     if (lane == 0)
       s_red[warp] = t;
@@ -400,30 +420,88 @@ __global__ void __launch_bounds__(kThreads)
       for (int w = 0; w < kWarps; w++)
         cta += s_red[w];
       ra.partials[blockIdx.x] = cta;
-      __threadfence();
-      s_last = atomicAdd(ra.ticket, 1) == (int)gridDim.x - 1;
     }
-    __syncthreads();
-    if (s_last) {
-      // The last CTA adds the per-CTA partials and the chunked-row slots with
-      // all its threads: fixed strided assignment, then a fixed-order tree.
-      __threadfence();
-      const int64_t total = (int64_t)gridDim.x + ra.nsplit;
-      double sum = 0.0;
-      for (int64_t i = threadIdx.x; i < total; i += kThreads)
-        sum += i < gridDim.x ? __ldcg(&ra.partials[i]) : __ldcg(&ra.rowres[i - gridDim.x]);
-      sum = wsum(sum);
-      if (lane == 0)
-        s_red[warp] = sum;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double t2 = 0.0;
-        for (int w = 0; w < kWarps; w++)
-          t2 += s_red[w];
-        *ra.out = t2;
-        *ra.ticket = 0;
-      }
+  }
+}
+
+// y of every split row whose first chunk lies in [c0, c1): its partials
+// added in chunk order (the order of the ticketed finish).
+template <class Acc, bool COMP>
+__global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64_t c1,
+                             const Acc *__restrict__ partials, Acc *__restrict__ y) {
+  const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += nth) {
+    const Chunk ch = chunks[c];
+    if (ch.first != c)
+      continue;
+    CSum<Acc> sum;
+    for (int i = 0; i < ch.count; i++) {
+      const Acc p = partials[ch.first + i];
+      if (COMP)
+        sum.add(p);
+      else
+        sum.s += p;
     }
+    y[ch.row] = sum.value();
+  }
+}
+
+// The fused row reduction's second pass: split rows as in chunk_finish, each
+// also adding its term to rowres[counter]; the last CTA (ticket) then adds
+// the main launch's per-CTA partials[0..main_grid) and rowres[0..nsplit) in
+// index order into *out.  Returns at once when the stop word is set.
+template <class Acc, bool COMP>
+__global__ void __launch_bounds__(kThreads)
+    resid_finish(const Chunk *__restrict__ chunks, int64_t nchunks,
+                 const Acc *__restrict__ cpart, Acc *__restrict__ y, WarpResid ra,
+                 int main_grid) {
+  __shared__ double s_red[kWarps];
+  __shared__ int s_last;
+  if (ra.stop && *static_cast<const volatile int *>(ra.stop))
+    return;
+  const Acc *bvec = static_cast<const Acc *>(ra.b);
+  const int64_t nth = (int64_t)gridDim.x * kThreads;
+  for (int64_t c = (int64_t)blockIdx.x * kThreads + threadIdx.x; c < nchunks; c += nth) {
+    const Chunk ch = chunks[c];
+    if (ch.first != c)
+      continue;
+    CSum<Acc> sum;
+    for (int i = 0; i < ch.count; i++) {
+      const Acc p = cpart[ch.first + i];
+      if (COMP)
+        sum.add(p);
+      else
+        sum.s += p;
+    }
+    const Acc v = sum.value();
+    y[ch.row] = v;
+    const double dd = (double)v - (double)bvec[ch.row];
+    ra.rowres[ch.counter] = ra.dot ? (double)v * (double)bvec[ch.row] : dd * dd;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(ra.ticket, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last)
+    return;
+  __threadfence();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t total = (int64_t)main_grid + ra.nsplit;
+  double sum = 0.0;
+  for (int64_t i = threadIdx.x; i < total; i += kThreads)
+    sum += i < main_grid ? __ldcg(&ra.partials[i]) : __ldcg(&ra.rowres[i - main_grid]);
+  sum = wsum(sum);
+  if (lane == 0)
+    s_red[warp] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t2 = 0.0;
+    for (int w = 0; w < kWarps; w++)
+      t2 += s_red[w];
+    *ra.out = t2;
+    *ra.ticket = 0;
   }
 }
 
@@ -452,12 +530,32 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
   WarpResid r{};
   if (ra)
     r = *ra;
+  DRB_CUDA_TRY(cudaMemsetAsync(P.counters.p, 0, sizeof(unsigned), s)); // work counter
   kern<<<grid, kThreads, 0, s>>>(A.rowptr.as<RI>(), A.colind.as<CI>(), A.vals.as<V>(),
                                  static_cast<const XT *>(x), static_cast<Acc *>(y),
                                  P.items.as<Item>(), P.nitems, P.chunks.as<Chunk>(),
                                  P.partials.as<Acc>(), P.counters.as<int>(), r);
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
+  if (RESID) {
+    const int g = (int)std::max<int64_t>(
+        1, std::min<int64_t>(148 * 4, (P.nchunks + kThreads - 1) / kThreads));
+    resid_finish<Acc, COMP><<<g, kThreads, 0, s>>>(P.chunks.as<Chunk>(), P.nchunks,
+                                                   P.partials.as<Acc>(),
+                                                   static_cast<Acc *>(y), r, grid);
+    note_launch();
+    DRB_CUDA_TRY(cudaGetLastError());
+  } else if (P.nchunks > 0) {
+    const int64_t c0 = P.fin_c1 >= 0 ? P.fin_c0 : 0;
+    const int64_t c1 = P.fin_c1 >= 0 ? P.fin_c1 : P.nchunks;
+    if (c1 > c0) {
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(148 * 4, (c1 - c0 + 255) / 256));
+      chunk_finish<Acc, COMP><<<g, 256, 0, s>>>(P.chunks.as<Chunk>(), c0, c1,
+                                                P.partials.as<Acc>(), static_cast<Acc *>(y));
+      note_launch();
+      DRB_CUDA_TRY(cudaGetLastError());
+    }
+  }
   return DRB_OK;
 }
 
