@@ -904,7 +904,10 @@ def profile_case(name):
       laplacian_f64  the single-RHS SpMV on the 2048^2 5-point Laplacian
                (4,194,304 rows, FP64 values, int32 indices; 335 MB);
       cg_f64   conjugate gradients on that Laplacian, FP64: one warm-up solve
-               of 8 iterations, then 24 iterations (rtol 0)."""
+               of 8 iterations, then 24 iterations (rtol 0);
+      powerlaw4m  the bench's SpMV kernel variant (256-nonzero items, plain
+               product layout) on the first 4,194,304 rows' worth of the bench
+               distribution (16,777,216 columns, so the same 64 MB x)."""
     import torch
     import drb
     from drb import mp
@@ -973,6 +976,18 @@ def profile_case(name):
         mp.conjugate_gradient(A, b, x, max_iters=8, rtol=0.0)
         x.zero_()
         mp.conjugate_gradient(A, b, x, max_iters=24, rtol=0.0)
+    elif name == "powerlaw4m":
+        os.environ["DRB_SPMV_VARIANT"] = "256,0"
+        alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
+        rp, ci, v = drb.gen.powerlaw_csr(4_194_304, N_COLS, alpha=alpha, hi=ZIPF_HI,
+                                         seed=SEED)
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (4_194_304, N_COLS)),
+                                         0, distr=mp.csr_row_distribution)
+        x = torch.from_numpy(drb.gen.values(N_COLS, seed=SEED + 1)).cuda()
+        y = torch.empty(4_194_304, device="cuda")
+        for _ in range(4):
+            A.gemv_device(x, y)
+        A.check()
     else:
         raise SystemExit(f"unknown profile case {name}")
     print("profile case", name, "done", flush=True)
@@ -993,7 +1008,8 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
-    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64", "cg_f64"],
+    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64", "cg_f64",
+                                                      "powerlaw4m"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
