@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(kAbarNT)
                 const Chunk *__restrict__ chunks) {
   __shared__ int64_t s_rp[kAbarSpan + 1];
   __shared__ uint16_t s_row[kAbarSpan]; // row (within the block) of each nonzero
+  __shared__ unsigned s_wmax[kAbarNT / 32];
   const int2 blk = blocks[blockIdx.x];
   const uint64_t pol_x = ptx::policy_evict_last();
   if (blk.y > 0) {
@@ -97,9 +98,49 @@ __global__ void __launch_bounds__(kAbarNT)
     const int64_t p0 = s_rp[0], p1 = s_rp[nrows];
     const bool stamped = p1 - p0 <= kAbarSpan && nrows <= 65536;
     if (stamped) {
+      // Every row writes its id at its first nonzero, then a block-wide
+      // running-max scan (row ids only grow along the nonzeros) gives every
+      // nonzero its row: 8 entries per thread whatever the row lengths
+      // (writing each row's ids by one thread serialised long rows).
+      constexpr int PER = kAbarSpan / kAbarNT;
+      const int span = (int)(p1 - p0);
+      for (int q = threadIdx.x; q < span; q += kAbarNT)
+        s_row[q] = 0;
+      __syncthreads();
       for (int i = threadIdx.x; i < nrows; i += kAbarNT)
-        for (int64_t p = s_rp[i]; p < s_rp[i + 1]; p++)
-          s_row[p - p0] = (uint16_t)i;
+        if (s_rp[i + 1] > s_rp[i])
+          s_row[s_rp[i] - p0] = (uint16_t)i;
+      __syncthreads();
+      const int q0 = threadIdx.x * PER;
+      unsigned v[PER];
+      unsigned run = 0;
+#pragma unroll
+      for (int k = 0; k < PER; k++) {
+        if (q0 + k < span)
+          run = max(run, (unsigned)s_row[q0 + k]);
+        v[k] = run;
+      }
+      // the running max of all threads before this one
+      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+      unsigned inc = run;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+          inc = max(inc, t);
+      }
+      if (lane == 31)
+        s_wmax[wid] = inc;
+      __syncthreads();
+      unsigned before = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0)
+        before = 0;
+      for (int w = 0; w < wid; w++)
+        before = max(before, s_wmax[w]);
+#pragma unroll
+      for (int k = 0; k < PER; k++)
+        if (q0 + k < span)
+          s_row[q0 + k] = (uint16_t)max(v[k], before);
     }
     __syncthreads();
     if (stamped) {
