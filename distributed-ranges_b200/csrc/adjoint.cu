@@ -8,14 +8,14 @@
 // each entry) and vals_t (values in CSC order).  A^T is then an ordinary CSR
 // matrix of shape n x m, so xbar uses the same row-block SpMV kernel as the
 // forward product: no atomics, fixed summation order.
-// abar walks the forward plan's row blocks so each entry's row is known
-// without an expanded row-index array.
+// abar runs on the forward product's work items, so each entry's row is
+// known without an expanded row-index array.
 #include <cub/device/device_radix_sort.cuh>
 
 #include <memory>
 #include <vector>
 
-#include "drb_internal.cuh"
+#include "spmv_warp.cuh"
 
 namespace drb {
 
@@ -73,127 +73,141 @@ __global__ void iota_kernel(T *out, int64_t n) {
     out[i] = (T)i;
 }
 
-constexpr int kAbarNT = 256;
-constexpr int kAbarSpan = 2048; // nonzeros of a row-block tile (the plan's tile)
+// abar on the forward product's work items (the persistent SpMV's plan):
+// warps take batches of 8 items from a work counter; per item, 16-byte loads
+// of the column indices, x gathered for all of them at once, the row of every
+// position stamped in a per-warp shared buffer (each row writes its index at
+// its first position, then a warp-wide running max fills the rest -- row
+// indices only grow along an item), and abar written with 16-byte stores.
+// Pure element-wise products: no sums, no order to keep.
+constexpr int kAbWarps = 8;
 
-// abar[p] = ybar[row(p)] * x[col(p)], one CTA per forward row block.
-template <class V, class CI, class RI>
-__global__ void __launch_bounds__(kAbarNT)
-    abar_kernel(const RI *__restrict__ rowptr, const CI *__restrict__ colind,
-                const V *__restrict__ ybar, const V *__restrict__ x,
-                V *__restrict__ abar, const int2 *__restrict__ blocks,
-                const Chunk *__restrict__ chunks) {
-  __shared__ int64_t s_rp[kAbarSpan + 1];
-  __shared__ uint16_t s_row[kAbarSpan]; // row (within the block) of each nonzero
-  __shared__ unsigned s_wmax[kAbarNT / 32];
-  const int2 blk = blocks[blockIdx.x];
+template <class V, class CI, class RI, int TILE>
+__global__ void __launch_bounds__(kAbWarps * 32)
+    abar_warp(const RI *__restrict__ rowptr, const CI *__restrict__ colind,
+              const V *__restrict__ ybar, const V *__restrict__ x, V *__restrict__ abar,
+              const Item *__restrict__ items, int64_t nitems, unsigned *counter, bool vec) {
+  constexpr int G = 16 / (sizeof(V) < sizeof(CI) ? sizeof(V) : sizeof(CI));
+  constexpr int NG = TILE / (G * 32);
+  constexpr int PER = (TILE + G + 31) / 32; // positions per lane in the row scan
+  constexpr int VPER = 16 / sizeof(V);
+  __shared__ uint8_t s_row[kAbWarps][PER * 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint8_t *srow = s_row[warp];
+  const uint64_t pol_s = ptx::policy_evict_first();
   const uint64_t pol_x = ptx::policy_evict_last();
-  if (blk.y > 0) {
-    // a tile of whole rows: rows stamp their nonzeros' row ids into shared
-    // memory, then all threads stream the nonzeros coalesced
-    const int r0 = blk.x, nrows = blk.y - blk.x;
-    for (int i = threadIdx.x; i <= nrows; i += kAbarNT)
-      s_rp[i] = (int64_t)rowptr[r0 + i];
-    __syncthreads();
-    const int64_t p0 = s_rp[0], p1 = s_rp[nrows];
-    const bool stamped = p1 - p0 <= kAbarSpan && nrows <= 65536;
-    if (stamped) {
-      // Every row writes its id at its first nonzero, then a block-wide
-      // running-max scan (row ids only grow along the nonzeros) gives every
-      // nonzero its row: 8 entries per thread whatever the row lengths
-      // (writing each row's ids by one thread serialised long rows).
-      constexpr int PER = kAbarSpan / kAbarNT;
-      const int span = (int)(p1 - p0);
-      for (int q = threadIdx.x; q < span; q += kAbarNT)
-        s_row[q] = 0;
-      __syncthreads();
-      for (int i = threadIdx.x; i < nrows; i += kAbarNT)
-        if (s_rp[i + 1] > s_rp[i])
-          s_row[s_rp[i] - p0] = (uint16_t)i;
-      __syncthreads();
-      const int q0 = threadIdx.x * PER;
+  constexpr int kBatch = 8;
+  auto grab = [&]() -> int64_t {
+    unsigned v = 0;
+    if (lane == 0)
+      v = atomicAdd(counter, (unsigned)kBatch);
+    return (int64_t)__shfl_sync(0xffffffffu, v, 0);
+  };
+  int64_t base = grab();
+  for (int k = 0;; k++) {
+    if (k == kBatch) {
+      base = grab();
+      k = 0;
+    }
+    const int64_t idx = base + k;
+    if (idx >= nitems)
+      break;
+    const Item it = warpk::load_item(items, idx);
+    const int64_t a0 = it.p0 & ~(int64_t)(G - 1);
+    const int off = (int)(it.p0 - a0), end = off + it.len;
+    const int ng = (end + G - 1) / G;
+    CI c[NG][G];
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+      if (g < ng)
+        warpk::ld_group<CI, G>(colind + a0 + (int64_t)g * G, c[j], pol_s);
+    }
+    V xv[NG][G];
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        const int q = g * G + i;
+        xv[j][i] = (g < ng && q >= off && q < end) ? ptx::ld_keep(x + c[j][i], pol_x) : V(0);
+      }
+    }
+    if (it.nrows > 0) {
+      for (int q = lane; q < end; q += 32)
+        srow[q] = 0;
+      __syncwarp();
+      for (int r = lane; r < it.nrows; r += 32) {
+        const int64_t b = (int64_t)rowptr[it.r0 + r] - a0;
+        const int64_t e = (int64_t)rowptr[it.r0 + r + 1] - a0;
+        if (e > b)
+          srow[b] = (uint8_t)r;
+      }
+      __syncwarp();
       unsigned v[PER];
       unsigned run = 0;
 #pragma unroll
-      for (int k = 0; k < PER; k++) {
-        if (q0 + k < span)
-          run = max(run, (unsigned)s_row[q0 + k]);
-        v[k] = run;
+      for (int t = 0; t < PER; t++) {
+        const int q = lane * PER + t;
+        if (q < end)
+          run = max(run, (unsigned)srow[q]);
+        v[t] = run;
       }
-      // the running max of all threads before this one
-      const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
       unsigned inc = run;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
-        const unsigned t = __shfl_up_sync(0xffffffffu, inc, o);
+        const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= o)
-          inc = max(inc, t);
+          inc = max(inc, u);
       }
-      if (lane == 31)
-        s_wmax[wid] = inc;
-      __syncthreads();
       unsigned before = __shfl_up_sync(0xffffffffu, inc, 1);
       if (lane == 0)
         before = 0;
-      for (int w = 0; w < wid; w++)
-        before = max(before, s_wmax[w]);
+      __syncwarp();
 #pragma unroll
-      for (int k = 0; k < PER; k++)
-        if (q0 + k < span)
-          s_row[q0 + k] = (uint16_t)max(v[k], before);
+      for (int t = 0; t < PER; t++) {
+        const int q = lane * PER + t;
+        if (q < end)
+          srow[q] = (uint8_t)max(v[t], before);
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    if (stamped) {
-      // all of this thread's nonzeros (at most kAbarSpan / kAbarNT) at once:
-      // column loads, then x gathers, then the products
-      constexpr int U = kAbarSpan / kAbarNT;
-      CI col[U];
-      V xv[U];
 #pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int64_t p = p0 + threadIdx.x + (int64_t)u * kAbarNT;
-        col[u] = p < p1 ? colind[p] : CI(0);
-      }
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+      if (g >= ng)
+        continue;
+      const int q0 = g * G;
+      V out[G];
 #pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int64_t p = p0 + threadIdx.x + (int64_t)u * kAbarNT;
-        xv[u] = p < p1 ? ptx::ld_keep(x + col[u], pol_x) : V(0);
+      for (int i = 0; i < G; i++) {
+        const int q = q0 + i;
+        if (q >= off && q < end) {
+          const int row = it.nrows > 0 ? (int)srow[q] : 0;
+          out[i] = ybar[it.r0 + row] * xv[j][i];
+        } else {
+          out[i] = V(0);
+        }
       }
+      V *dst = abar + a0 + q0;
+      if (vec && q0 >= off && q0 + G <= end) {
 #pragma unroll
-      for (int u = 0; u < U; u++) {
-        const int64_t p = p0 + threadIdx.x + (int64_t)u * kAbarNT;
-        if (p < p1)
-          abar[p] = ybar[r0 + s_row[p - p0]] * xv[u];
+        for (int h = 0; h < G / VPER; h++) {
+          warpk::Vec16<V> w;
+#pragma unroll
+          for (int i = 0; i < VPER; i++)
+            w.t[i] = out[h * VPER + i];
+          *reinterpret_cast<uint4 *>(dst + h * VPER) = w.u;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < G; i++)
+          if (q0 + i >= off && q0 + i < end)
+            dst[i] = out[i];
       }
-      return;
     }
-    for (int64_t p = p0 + threadIdx.x; p < p1; p += kAbarNT) {
-      int lo = 0, hi = nrows; // last i with s_rp[i] <= p
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (s_rp[mid] <= p)
-          lo = mid;
-        else
-          hi = mid;
-      }
-      abar[p] = ybar[r0 + lo] * ptx::ld_keep(x + colind[p], pol_x);
-    }
-    return;
+    __syncwarp(); // srow is rewritten by the next item
   }
-  int64_t row, lo, hi;
-  if (blk.y == -1) {
-    row = blk.x;
-    lo = (int64_t)rowptr[row];
-    hi = (int64_t)rowptr[row + 1];
-  } else {
-    const Chunk ch = chunks[-blk.y - 2];
-    row = ch.row;
-    lo = ch.p0;
-    hi = ch.p1;
-  }
-  const V yb = ybar[row];
-  for (int64_t p = lo + threadIdx.x; p < hi; p += kAbarNT)
-    abar[p] = yb * ptx::ld_keep(x + colind[p], pol_x);
 }
 
 unsigned grid1(int64_t n) {
@@ -304,17 +318,37 @@ drb_status build_v(Csr &A, cudaStream_t s) {
   return build_typed<V, int64_t, int64_t>(A, s);
 }
 
-template <class V, class CI, class RI>
-drb_status abar_typed(Csr &A, const V *ybar, const V *x, V *abar,
-                      cudaStream_t s) {
-  if (A.plan.nblocks == 0)
-    return DRB_OK;
-  abar_kernel<V, CI, RI><<<(unsigned)A.plan.nblocks, kAbarNT, 0, s>>>(
-      A.rowptr.as<RI>(), A.colind.as<CI>(), ybar, x, abar,
-      A.plan.blocks.as<int2>(), A.plan.chunks.as<Chunk>());
+template <class V, class CI, class RI, int TILE>
+drb_status abar_tile(Csr &A, const V *ybar, const V *x, V *abar, cudaStream_t s) {
+  static int grid_cache[64] = {0};
+  int &grid = grid_cache[A.device < 64 ? A.device : 0];
+  if (grid == 0) {
+    int occ = 0, sms = 0;
+    DRB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, abar_warp<V, CI, RI, TILE>, kAbWarps * 32, 0));
+    DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
+    grid = std::max(1, occ) * sms;
+  }
+  const PipePlan &P = A.pipe;
+  const int g = (int)std::min<int64_t>(grid, (P.nitems + kAbWarps - 1) / kAbWarps);
+  const bool vec = reinterpret_cast<uintptr_t>(abar) % 16 == 0;
+  DRB_CUDA_TRY(cudaMemsetAsync(P.counters.p, 0, sizeof(unsigned), s)); // work counter
+  abar_warp<V, CI, RI, TILE><<<g, kAbWarps * 32, 0, s>>>(
+      A.rowptr.as<RI>(), A.colind.as<CI>(), ybar, x, abar, P.items.as<Item>(), P.nitems,
+      P.counters.as<unsigned>(), vec);
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
   return DRB_OK;
+}
+
+template <class V, class CI, class RI>
+drb_status abar_typed(Csr &A, const V *ybar, const V *x, V *abar,
+                      cudaStream_t s) {
+  if (A.pipe.nitems == 0)
+    return DRB_OK;
+  if (A.pipe.tile == 512)
+    return abar_tile<V, CI, RI, 512>(A, ybar, x, abar, s);
+  return abar_tile<V, CI, RI, 256>(A, ybar, x, abar, s);
 }
 
 template <class V>
@@ -387,6 +421,10 @@ drb_status spmv_t_launch(Csr &A, const void *ybar, void *xbar, cudaStream_t s) {
 
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
                        cudaStream_t s) {
+  // short regular rows: the sliced copy's lane-per-row layout (per-item row
+  // stamping costs more than the products on 5-nonzero rows)
+  if (A.sell.on && sell_abar_launch(A, ybar, x, abar, s) == DRB_OK)
+    return DRB_OK;
   if (A.storage == DRB_F32)
     return abar_v<float>(A, ybar, x, abar, s);
   if (A.storage == DRB_F64)

@@ -238,6 +238,10 @@ drb_status pipe_check(Csr &A, cudaStream_t s);
 drb_status sell_build(Csr &A, const void *rowptr_host, int rbytes, cudaStream_t s);
 void sell_release(Csr &A);
 drb_status sell_pack_values(Csr &A, cudaStream_t s); // after the CSR values change
+// abar = ybar_i * x_j on the sliced copy (short regular rows); returns
+// DRB_ERR_UNSUPPORTED without launching when the copy is off or too wide.
+drb_status sell_abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
+                            cudaStream_t s);
 namespace warpk {
 struct WarpResid;
 }
