@@ -492,11 +492,13 @@ namespace {
 
 constexpr int kHostSegments = 6;          // row segments of a host-pointer gemv
 constexpr int64_t kSegmentMinNnz = 1 << 22; // below this, one launch
-// Each segment holds this fraction of the previous one's nonzeros: y's copy
-// back over PCIe runs at about 0.6x the rate the kernel produces it, so each
-// segment's copy ends about when the next segment's compute does, and the
-// small last segment leaves a short tail.
-constexpr double kSegmentRatio = 0.6;
+// Each segment holds this fraction of the previous one's nonzeros, so each
+// segment's copy back over PCIe ends about when the next segment's compute
+// does and the small last segment leaves a short tail.  Measured on a 16.8M-row
+// power-law matrix (64 MB of y, 1.18 ms D2H against 1.55 ms of SpMV): 6
+// segments at 0.6 / 0.7 / 0.8: 3.14 / 3.08 / 3.11 ms per call; 8 to 16
+// segments 3.12 to 3.43 ms (each launch adds a ramp and a tail).
+constexpr double kSegmentRatio = 0.7;
 
 // Segment count of a host-pointer gemv: DRB_HOST_SEGMENTS (1..64) when set,
 // read when a handle first runs one.
@@ -505,6 +507,15 @@ int host_segments() {
   if (!e || !*e)
     return kHostSegments;
   return std::min(64, std::max(1, std::atoi(e)));
+}
+
+// Ratio of consecutive segments' nnz: DRB_HOST_SEGMENT_RATIO (0.2..1) when
+// set, read with the segment count.
+double segment_ratio() {
+  const char *e = std::getenv("DRB_HOST_SEGMENT_RATIO");
+  if (!e || !*e)
+    return kSegmentRatio;
+  return std::min(1.0, std::max(0.2, std::atof(e)));
 }
 
 // Orders the single-RHS items by row and cuts them into at most `target` row
@@ -523,11 +534,12 @@ drb_status build_row_segments(Csr &A, int target) {
     total += t.len;
   // cut[j]: running nnz at which segment j + 1 may start
   std::vector<double> cut;
+  const double ratio = segment_ratio();
   double w = 1.0, wsum = 0.0;
-  for (int j = 0; j < target; j++, w *= kSegmentRatio)
+  for (int j = 0; j < target; j++, w *= ratio)
     wsum += w;
   w = 1.0;
-  for (double acc = 0.0; (int)cut.size() < target - 1; w *= kSegmentRatio) {
+  for (double acc = 0.0; (int)cut.size() < target - 1; w *= ratio) {
     acc += w;
     cut.push_back((double)total * acc / wsum);
   }
@@ -568,13 +580,14 @@ drb_status build_row_segments(Csr &A, int target) {
 void build_slice_segments(Csr &A, int target) {
   const std::vector<int64_t> &off = A.sell.off_h;
   const int64_t nsl = A.sell.nslices, total = off[nsl];
+  const double ratio = segment_ratio();
   double w = 1.0, wsum = 0.0;
-  for (int j = 0; j < target; j++, w *= kSegmentRatio)
+  for (int j = 0; j < target; j++, w *= ratio)
     wsum += w;
   A.sell.seg_s0.assign(1, 0);
   w = 1.0;
   double acc = 0.0;
-  for (int j = 0; j < target - 1; j++, w *= kSegmentRatio) {
+  for (int j = 0; j < target - 1; j++, w *= ratio) {
     acc += w;
     const double cut = (double)total * acc / wsum;
     int64_t sl = std::lower_bound(off.begin(), off.end(), (int64_t)cut) - off.begin();

@@ -133,15 +133,19 @@ __device__ __forceinline__ Item load_item(const Item *items, int64_t i) {
 __device__ __forceinline__ int skew(int q) { return q + (q >> 5); }
 
 // Fused row reduction: ||A x - b||^2, or with `dot` set sum_i y_i b_i (b is
-// then a weight vector, e.g. p for p.Ap).  Whole rows add into a per-CTA
-// partial; a chunked row's term goes to its own slot rowres[counter],
-// written by the finish pass, whose last CTA sums partials[0..grid) then
-// rowres[0..nsplit) in order.  A non-null `stop` pointing at a non-zero word
-// makes the launches return before touching anything (a converged iterative
-// loop replaying a captured graph).
+// then a weight vector, e.g. p for p.Ap).  The whole rows of work item i add
+// into their own slot ipart[i] (whichever warp ran the item); a chunked row's
+// term goes to its own slot rowres[counter], written by the finish pass.  The
+// finish pass's CTAs sum fixed ranges of ipart into partials[cta] and its
+// last CTA sums partials[0..grid) then rowres[0..nsplit) in order, so the
+// result never depends on the schedule.  (The sliced-ELL kernel writes one
+// partial per CTA and combines them itself.)  A non-null `stop` pointing at
+// a non-zero word makes the launches return before touching anything (a
+// converged iterative loop replaying a captured graph).
 struct WarpResid {
   const void *b = nullptr;
   double *partials = nullptr;
+  double *ipart = nullptr;
   double *rowres = nullptr;
   int64_t nsplit = 0;
   int *ticket = nullptr;
@@ -350,7 +354,6 @@ __global__ void __launch_bounds__(kThreads)
   using Acc = typename AccOf<V>::type;
   __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
   __shared__ int s_rp[kWarps][kRows + 1];
-  __shared__ double s_red[kWarps];
 
   if (RESID && ra.stop && *static_cast<const volatile int *>(ra.stop))
     return; // uniform: every CTA reads the same word, written by an earlier launch
@@ -364,63 +367,44 @@ __global__ void __launch_bounds__(kThreads)
   Acc *prod = s_prod[warp];
   int *srp = s_rp[warp];
 
-  // The plain product takes items in batches of kBatch consecutive indices
-  // from a work counter (zeroed before the launch; lane 0 takes the next
-  // index one item ahead, so the atomic's round trip overlaps the current
-  // item): a fixed round-robin share was sensitive to the exact sequence of
-  // item costs (the bench's power-law ran 2.23 ms against 1.61 ms for the
-  // same distribution with another seed; batched grabs: 1.53 ms for both).
-  // Which warp runs an item does not change any row's sum.  A fused row
-  // reduction adds rows into per-CTA partials, whose grouping would then
-  // vary run to run, so it keeps the fixed share (warp w: items w, w + W,
-  // ...) and stays deterministic.
-  if (RESID) {
-    const int64_t nw = (int64_t)gridDim.x * kWarps;
-    int64_t it = (int64_t)blockIdx.x * kWarps + warp;
-    Slot<V, CI, TILE> A;
-    K.fetch(A, it);
-    while (A.valid) {
-      K.template process<RESID>(A, it + nw, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
-      it += nw;
-    }
-  } else {
-    constexpr int kBatch = 8; // items per grab
-    auto grab = [&]() -> int64_t {
-      unsigned v = 0;
-      if (lane == 0)
-        v = atomicAdd(reinterpret_cast<unsigned *>(counters), (unsigned)kBatch);
-      return (int64_t)__shfl_sync(0xffffffffu, v, 0);
-    };
-    int64_t base = grab();
-    int k = 0;
-    auto advance = [&]() -> int64_t {
-      if (++k == kBatch) {
-        base = grab();
-        k = 0;
-      }
-      return base + k;
-    };
-    Slot<V, CI, TILE> A;
-    K.fetch(A, base);
-    int64_t next = advance();
-    while (A.valid) {
-      K.template process<RESID>(A, next, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
-      next = advance();
-    }
-  }
-
-  if (RESID) {
-    // the CTA's partial; resid_finish adds the split rows and combines
-    const double t = wsum(r2);
+  // Warps take items in batches of kBatch consecutive indices from a work
+  // counter (zeroed before the launch; lane 0 takes the next index one item
+  // ahead, so the atomic's round trip overlaps the current item): a fixed
+  // round-robin share was sensitive to the exact sequence of item costs (the
+  // bench's power-law ran 2.23 ms against 1.61 ms for the same distribution
+  // with another seed; batched grabs: 1.53 ms for both).  Which warp runs an
+  // item changes neither a row's sum nor an item's reduction slot.
+  constexpr int kBatch = 8; // items per grab
+  auto grab = [&]() -> int64_t {
+    unsigned v = 0;
     if (lane == 0)
-      s_red[warp] = t;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double cta = 0.0;
-      for (int w = 0; w < kWarps; w++)
-        cta += s_red[w];
-      ra.partials[blockIdx.x] = cta;
+      v = atomicAdd(reinterpret_cast<unsigned *>(counters), (unsigned)kBatch);
+    return (int64_t)__shfl_sync(0xffffffffu, v, 0);
+  };
+  int64_t base = grab();
+  int k = 0;
+  auto advance = [&]() -> int64_t {
+    if (++k == kBatch) {
+      base = grab();
+      k = 0;
     }
+    return base + k;
+  };
+  Slot<V, CI, TILE> A;
+  int64_t cur = base;
+  K.fetch(A, cur);
+  int64_t next = advance();
+  while (A.valid) {
+    K.template process<RESID>(A, next, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
+    if (RESID) {
+      // the item's whole rows, in row order within each lane, then a fixed tree
+      const double t = wsum(r2);
+      if (lane == 0)
+        ra.ipart[cur] = t;
+      r2 = 0.0;
+    }
+    cur = next;
+    next = advance();
   }
 }
 
@@ -447,14 +431,15 @@ __global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64
 }
 
 // The fused row reduction's second pass: split rows as in chunk_finish, each
-// also adding its term to rowres[counter]; the last CTA (ticket) then adds
-// the main launch's per-CTA partials[0..main_grid) and rowres[0..nsplit) in
-// index order into *out.  Returns at once when the stop word is set.
+// also adding its term to rowres[counter]; CTA b sums the item slots
+// ipart[b * per, (b + 1) * per) into partials[b]; the last CTA (ticket) then
+// adds partials[0..grid) and rowres[0..nsplit) in index order into *out.
+// Returns at once when the stop word is set.
 template <class Acc, bool COMP>
 __global__ void __launch_bounds__(kThreads)
     resid_finish(const Chunk *__restrict__ chunks, int64_t nchunks,
                  const Acc *__restrict__ cpart, Acc *__restrict__ y, WarpResid ra,
-                 int main_grid) {
+                 int64_t nitems) {
   __shared__ double s_red[kWarps];
   __shared__ int s_last;
   if (ra.stop && *static_cast<const volatile int *>(ra.stop))
@@ -478,6 +463,24 @@ __global__ void __launch_bounds__(kThreads)
     const double dd = (double)v - (double)bvec[ch.row];
     ra.rowres[ch.counter] = ra.dot ? (double)v * (double)bvec[ch.row] : dd * dd;
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  {
+    const int64_t per = (nitems + gridDim.x - 1) / gridDim.x;
+    const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(nitems, i0 + per);
+    double sum = 0.0;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += kThreads)
+      sum += ra.ipart[i];
+    sum = wsum(sum);
+    if (lane == 0)
+      s_red[warp] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double cta = 0.0;
+      for (int w = 0; w < kWarps; w++)
+        cta += s_red[w];
+      ra.partials[blockIdx.x] = cta;
+    }
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -487,12 +490,12 @@ __global__ void __launch_bounds__(kThreads)
   if (!s_last)
     return;
   __threadfence();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t total = (int64_t)main_grid + ra.nsplit;
+  const int64_t np = gridDim.x, total = np + ra.nsplit;
   double sum = 0.0;
   for (int64_t i = threadIdx.x; i < total; i += kThreads)
-    sum += i < main_grid ? __ldcg(&ra.partials[i]) : __ldcg(&ra.rowres[i - main_grid]);
+    sum += i < np ? __ldcg(&ra.partials[i]) : __ldcg(&ra.rowres[i - np]);
   sum = wsum(sum);
+  __syncthreads(); // s_red is reused
   if (lane == 0)
     s_red[warp] = sum;
   __syncthreads();
@@ -504,6 +507,10 @@ __global__ void __launch_bounds__(kThreads)
     *ra.ticket = 0;
   }
 }
+
+// Upper bound on resid_finish's grid (its per-CTA partials live in the
+// fused-reduction scratch).
+constexpr int kResidFinishGrid = 592;
 
 struct Shape {
   int grid = 0;
@@ -538,11 +545,14 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
   if (RESID) {
+    // a function of the plan only, so the reduction's grouping is fixed
     const int g = (int)std::max<int64_t>(
-        1, std::min<int64_t>(148 * 4, (P.nchunks + kThreads - 1) / kThreads));
+        1, std::min<int64_t>(kResidFinishGrid,
+                             std::max((P.nchunks + kThreads - 1) / kThreads,
+                                      (P.nitems + 8191) / 8192)));
     resid_finish<Acc, COMP><<<g, kThreads, 0, s>>>(P.chunks.as<Chunk>(), P.nchunks,
                                                    P.partials.as<Acc>(),
-                                                   static_cast<Acc *>(y), r, grid);
+                                                   static_cast<Acc *>(y), r, P.nitems);
     note_launch();
     DRB_CUDA_TRY(cudaGetLastError());
   } else if (P.nchunks > 0) {

@@ -406,6 +406,26 @@ def test_residual_norm2(mp, dtype):
         1e-5 if dtype == np.float32 else 1e-12)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_residual_norm2_repeatable_with_dynamic_schedule(mp, dtype):
+    """Warps take work items dynamically, so which warp runs an item changes
+    from launch to launch; each item's rows reduce into the item's own slot and
+    the slots are summed in a fixed order, so ||Ax - b||^2 repeats bit for bit."""
+    import drb
+    m = n = 300_000
+    rp, ci, v = drb.gen.powerlaw_csr(m, n, alpha=1.76, hi=8192, seed=11)
+    v = v.astype(dtype)
+    rng = np.random.default_rng(3)
+    x = torch.from_numpy(rng.uniform(-1, 1, n).astype(dtype)).cuda()
+    b = torch.from_numpy(rng.uniform(-1, 1, m).astype(dtype)).cuda()
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    y = torch.empty(m, dtype=x.dtype, device="cuda")
+    outs = [mp.residual_norm2(a, x, b, y).item() for _ in range(6)]
+    assert len(set(outs)) == 1
+    ref = float(((y.double() - b.double()) ** 2).sum())
+    assert abs(outs[0] - ref) <= 1e-10 * ref
+
+
 # ---- adjoint ------------------------------------------------------------------------
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("kind", ["chunky", "laplacian"])
