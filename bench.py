@@ -277,6 +277,14 @@ def run_ours(args):
     e2e_val = world * bytes_ / e2e_s / 1e9
     assert np.array_equal(yh.numpy(), yd.cpu().numpy())
 
+    # the streaming-gather floor on this pattern (column indices and values
+    # streamed, x gathered at each, no rows): the roofline of a gather-bound SpMV
+    mp.gather_probe(A, xd)
+    probe_ms = statistics.mean(timed_launches(lambda: mp.gather_probe(A, xd), args.steps, stream))
+    mp.gather_probe(A, xd, False)
+    probe_cols_ms = statistics.mean(timed_launches(lambda: mp.gather_probe(A, xd, False),
+                                                   args.steps, stream))
+
     extra = {}
     if not args.no_extra:
         extra = extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes_, kern_ms, stream)
@@ -320,6 +328,13 @@ def run_ours(args):
                                      "clock (288 G/s measured on this B200)",
                              "ceiling_GBps": round(288e9 * bytes_ / nnz / 1e9, 1),
                              "frac": round(achieved / (288e9 * bytes_ / nnz / 1e9), 4)},
+                         "stream_gather_floor": {
+                             "what": "drb_csr_gather_probe on this matrix: column indices and "
+                                     "values streamed with the SpMV's loads, x gathered at "
+                                     "each, no rows or y (measured in this run)",
+                             "ms": round(probe_ms, 4),
+                             "ms_indices_only": round(probe_cols_ms, 4),
+                             "frac": round(probe_ms / kern_ms, 4)},
                          "alg_bytes_per_launch": bytes_,
                          "kernel_ms": round(kern_ms, 4)},
             "cpu_baseline": cpu,
@@ -394,6 +409,30 @@ def extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes32, fwd_ms, stream):
                      "frac": round(db / (ms * 1e-3) / 1e9 / peak, 4),
                      "gflops": round(2 * n * n / (ms * 1e-3) / 1e9, 2)}
         del Ad, xv, yv
+    torch.cuda.empty_cache()
+
+    # dot / squared norm: 2 x 2 GB streamed, f64 accumulation, fixed order
+    for name, dt, eb in (("dot_fp32", torch.float32, 4), ("dot_fp64", torch.float64, 8)):
+        n = (1 << 31) // eb
+        g = torch.Generator(device="cuda").manual_seed(SEED + 12)
+        av = torch.empty(n, device="cuda", dtype=dt).uniform_(-1, 1, generator=g)
+        bv = torch.empty(n, device="cuda", dtype=dt).uniform_(-1, 1, generator=g)
+        res = torch.empty(1, device="cuda", dtype=torch.float64)
+        mp.dot(av, bv, res)
+        ms = statistics.mean(timed_launches(lambda: mp.dot(av, bv, res), steps, stream))
+        db = 2 * eb * n
+        out[name] = {"n": n, "ms": round(ms, 4), "GBps": round(db / (ms * 1e-3) / 1e9, 2),
+                     "frac": round(db / (ms * 1e-3) / 1e9 / peak, 4)}
+        if name == "dot_fp32":
+            # mp::reduce (sum) over a 2 GB distributed_vector's storage
+            res32 = torch.empty(1, device="cuda", dtype=torch.float32)
+            mp.reduce(av, out=res32)
+            ms = statistics.mean(timed_launches(lambda: mp.reduce(av, out=res32), steps,
+                                                stream))
+            out["reduce_sum_fp32"] = {"n": n, "ms": round(ms, 4),
+                                      "GBps": round(4 * n / (ms * 1e-3) / 1e9, 2),
+                                      "frac": round(4 * n / (ms * 1e-3) / 1e9 / peak, 4)}
+        del av, bv
     torch.cuda.empty_cache()
     return out
 
@@ -908,7 +947,9 @@ def profile_case(name):
                of 8 iterations, then 24 iterations (rtol 0);
       powerlaw4m  the bench's SpMV kernel variant (256-nonzero items, plain
                product layout) on the first 4,194,304 rows' worth of the bench
-               distribution (16,777,216 columns, so the same 64 MB x)."""
+               distribution (16,777,216 columns, so the same 64 MB x);
+      residual4m  the fused ||Ax - b||^2 on that matrix (same variant);
+      dot_f32  the dot kernel on two FP32 vectors of 2^26 elements (2 x 256 MB)."""
     import torch
     import drb
     from drb import mp
@@ -977,7 +1018,7 @@ def profile_case(name):
         mp.conjugate_gradient(A, b, x, max_iters=8, rtol=0.0)
         x.zero_()
         mp.conjugate_gradient(A, b, x, max_iters=24, rtol=0.0)
-    elif name == "powerlaw4m":
+    elif name in ("powerlaw4m", "residual4m"):
         os.environ["DRB_SPMV_VARIANT"] = "256,0"
         alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
         rp, ci, v = drb.gen.powerlaw_csr(4_194_304, N_COLS, alpha=alpha, hi=ZIPF_HI,
@@ -986,9 +1027,21 @@ def profile_case(name):
                                          0, distr=mp.csr_row_distribution)
         x = torch.from_numpy(drb.gen.values(N_COLS, seed=SEED + 1)).cuda()
         y = torch.empty(4_194_304, device="cuda")
+        b = torch.from_numpy(drb.gen.values(4_194_304, seed=SEED + 2)).cuda()
         for _ in range(4):
-            A.gemv_device(x, y)
+            if name == "powerlaw4m":
+                A.gemv_device(x, y)
+            else:
+                mp.residual_norm2(A, x, b, y)
         A.check()
+    elif name == "dot_f32":
+        g = torch.Generator(device="cuda").manual_seed(SEED + 12)
+        a = torch.empty(1 << 26, device="cuda").uniform_(-1, 1, generator=g)
+        b = torch.empty(1 << 26, device="cuda").uniform_(-1, 1, generator=g)
+        out = torch.empty(1, device="cuda", dtype=torch.float64)
+        for _ in range(4):
+            mp.dot(a, b, out)
+        torch.cuda.synchronize()
     else:
         raise SystemExit(f"unknown profile case {name}")
     print("profile case", name, "done", flush=True)
@@ -1009,8 +1062,8 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
-    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64", "cg_f64",
-                                                      "powerlaw4m"],
+    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64",
+                                               "cg_f64", "powerlaw4m", "residual4m", "dot_f32"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:

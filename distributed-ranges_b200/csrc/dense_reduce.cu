@@ -313,7 +313,8 @@ drb_status dense_typed(int64_t m, int64_t n, const V *A, int64_t lda,
 
 // ---- dot -------------------------------------------------------------------------
 constexpr int kDotNT = 256;
-constexpr int kDotGrid = 296; // fixed: the summation order must not vary
+constexpr int kDotGrid = 592; // fixed: the summation order must not vary
+constexpr int kDotUnroll = 4; // 16-byte loads in flight per vector per thread
 
 template <class V>
 __global__ void __launch_bounds__(kDotNT)
@@ -330,12 +331,29 @@ __global__ void __launch_bounds__(kDotNT)
                    (reinterpret_cast<uintptr_t>(b) % 16 == 0);
   int64_t done = 0;
   if (vec) {
+    union W {
+      uint4 u;
+      V t[PER];
+    };
     const int64_t nv = n / PER;
-    for (int64_t i = tid; i < nv; i += nth) {
-      union {
-        uint4 u;
-        V t[PER];
-      } wa, wb;
+    int64_t i = tid;
+    // kDotUnroll grid-strided vectors per trip, all loads issued first
+    for (; i + (kDotUnroll - 1) * nth < nv; i += kDotUnroll * nth) {
+      W wa[kDotUnroll], wb[kDotUnroll];
+#pragma unroll
+      for (int u = 0; u < kDotUnroll; u++)
+        wa[u].u = ptx::ld_stream16(a + (i + u * nth) * PER, pol_s);
+#pragma unroll
+      for (int u = 0; u < kDotUnroll; u++)
+        wb[u].u = (a == b) ? wa[u].u : ptx::ld_stream16(b + (i + u * nth) * PER, pol_s);
+#pragma unroll
+      for (int u = 0; u < kDotUnroll; u++)
+#pragma unroll
+        for (int q = 0; q < PER; q++)
+          acc += (double)wa[u].t[q] * (double)wb[u].t[q];
+    }
+    for (; i < nv; i += nth) {
+      W wa, wb;
       wa.u = ptx::ld_stream16(a + i * PER, pol_s);
       wb.u = (a == b) ? wa.u : ptx::ld_stream16(b + i * PER, pol_s);
 #pragma unroll

@@ -27,7 +27,8 @@ namespace drb {
 namespace {
 
 constexpr int kRedNT = 256;
-constexpr int kRedGrid = 296; // fixed: the grouping must not depend on the GPU
+constexpr int kRedGrid = 592; // fixed: the grouping must not depend on the GPU
+constexpr int kRedUnroll = 4; // 16-byte loads in flight per thread
 
 template <class T> struct SumAcc { using type = T; };
 template <> struct SumAcc<float> { using type = double; };
@@ -100,11 +101,25 @@ __global__ void __launch_bounds__(kRedNT)
     head = head < n ? head : n;
     const int64_t nv = (n - head) / PER;
     const T *xa = x + head;
-    for (int64_t i = tid; i < nv; i += nth) {
-      union {
-        uint4 u;
-        T t[PER];
-      } w;
+    union W {
+      uint4 u;
+      T t[PER];
+    };
+    int64_t i = tid;
+    // kRedUnroll grid-strided vectors per trip, all loads issued first
+    for (; i + (kRedUnroll - 1) * nth < nv; i += kRedUnroll * nth) {
+      W w[kRedUnroll];
+#pragma unroll
+      for (int u = 0; u < kRedUnroll; u++)
+        w[u].u = ptx::ld_stream16(xa + (i + u * nth) * PER, pol);
+#pragma unroll
+      for (int u = 0; u < kRedUnroll; u++)
+#pragma unroll
+        for (int q = 0; q < PER; q++)
+          acc = R::f(acc, R::lift(w[u].t[q]));
+    }
+    for (; i < nv; i += nth) {
+      W w;
       w.u = ptx::ld_stream16(xa + i * PER, pol);
 #pragma unroll
       for (int q = 0; q < PER; q++)

@@ -173,6 +173,16 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
  * kernel then skipped the rest of its work; the error word is cleared). */
 drb_status drb_csr_check(drb_csr_t A, void *stream);
 
+/* Measurement only; no counterpart in the reference.  Streams A's column
+ * indices (and its values when with_values != 0) with the SpMV's 16-byte
+ * loads and gathers x[col] at every nonzero: the reads of y = A x without
+ * rows, row sums or y, so its time is a floor for any SpMV on this pattern
+ * that fetches x element by element (random columns make that, not HBM, the
+ * bound).  Writes nothing the caller sees.  F32 or F64 storage; x: device,
+ * n elements of the value type. */
+drb_status drb_csr_gather_probe(drb_csr_t A, const void *x, int with_values,
+                                void *stream);
+
 /* Fused residual: out[0] = || A*x - b ||_2^2 accumulated in f64 (device
  * double*), y = A*x also written when y != NULL.  k = 1. */
 drb_status drb_csr_residual_norm2(drb_csr_t A, const void *x, const void *b,

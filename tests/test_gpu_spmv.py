@@ -426,6 +426,32 @@ def test_residual_norm2_repeatable_with_dynamic_schedule(mp, dtype):
     assert abs(outs[0] - ref) <= 1e-10 * ref
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("index", [np.int32, np.int64])
+def test_gather_probe_runs_and_checks_storage(mp, dtype, index):
+    """The measurement-only gather probe reads a handle's columns (and values)
+    and x without writing anything visible; BF16 storage is refused."""
+    from drb import _capi as capi
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp.astype(index), ci.astype(index),
+                                                        (m, n)), 0)
+    x = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, n).astype(dtype)).cuda()
+    y0 = torch.empty(m, dtype=x.dtype, device="cuda")
+    a.gemv_device(x, y0)
+    x0 = x.clone()
+    mp.gather_probe(a, x)
+    mp.gather_probe(a, x, with_values=False)
+    y1 = torch.empty_like(y0)
+    a.gemv_device(x, y1)
+    assert torch.equal(x, x0) and torch.equal(y0, y1)
+    a.check()
+    vb = v.astype(np.float32)
+    b16 = mp.distributed_sparse_matrix(mp.csr_matrix_view(vb, rp, ci, (m, n)), 0,
+                                       storage=torch.bfloat16)
+    rc = capi.lib.drb_csr_gather_probe(b16.handle, C.c_void_p(x.data_ptr()), 1, None)
+    assert rc == capi.DRB_ERR_UNSUPPORTED
+
+
 # ---- adjoint ------------------------------------------------------------------------
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("kind", ["chunky", "laplacian"])
