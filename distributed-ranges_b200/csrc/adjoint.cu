@@ -8,8 +8,10 @@
 // each entry) and vals_t (values in CSC order).  A^T is then an ordinary CSR
 // matrix of shape n x m, so xbar uses the same row-block SpMV kernel as the
 // forward product: no atomics, fixed summation order.
-// abar runs on the forward product's work items, so each entry's row is
-// known without an expanded row-index array.
+// abar needs each entry's row without an expanded row-index array: short
+// rows (at most 64 nonzeros) find it by a warp-wide search over 32 row starts
+// (abar_rows), longer rows run on the forward product's work items
+// (abar_warp).
 #include <cub/device/device_radix_sort.cuh>
 
 #include <memory>
@@ -318,6 +320,103 @@ drb_status build_v(Csr &A, cudaStream_t s) {
   return build_typed<V, int64_t, int64_t>(A, s);
 }
 
+// Abar for short rows (at most kAbRowsMaxLen nonzeros): a warp takes 32
+// consecutive rows; lane l holds rowptr[r0 + l] (relative to the group's
+// first nonzero) and ybar[r0 + l].  The warp walks the group's nonzeros 32
+// at a time: each lane loads its position's column (coalesced), gathers x,
+// finds the position's row by a 5-step binary search over the lanes' row
+// starts (shuffles) and takes that row's ybar with one more shuffle, then
+// stores abar (coalesced).  No shared memory and no per-item bookkeeping, so
+// rows of a handful of nonzeros (a stencil) stream at close to HBM speed.
+constexpr int kAbRowsNT = 256;
+constexpr int kAbRowsMaxLen = 64; // a group spans at most 32 * 64 nonzeros
+
+template <class V, class CI, class RI>
+__global__ void __launch_bounds__(kAbRowsNT)
+    abar_rows(int64_t m, const RI *__restrict__ rowptr, const CI *__restrict__ colind,
+              const V *__restrict__ ybar, const V *__restrict__ x, V *__restrict__ abar) {
+  // U positions per lane per trip with all loads first; the last partial
+  // trip goes 32 positions at a time (a masked U-wide trip measured slower:
+  // 2048^2 Laplacian FP32 0.064 against 0.0485 ms)
+  constexpr int U = 4;
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * kAbRowsNT) >> 5;
+  const uint64_t pol_x = ptx::policy_evict_last();
+  for (int64_t r0 = (((int64_t)blockIdx.x * kAbRowsNT + threadIdx.x) >> 5) * 32; r0 < m;
+       r0 += nw * 32) {
+    const int64_t r = r0 + lane;
+    const int64_t pbeg = (int64_t)rowptr[r0];
+    const int64_t pend = (int64_t)rowptr[r0 + 32 < m ? r0 + 32 : m];
+    // rows past m start at the group's end: never selected
+    const int rs = (int)((int64_t)rowptr[r < m ? r : m] - pbeg);
+    const V yb = r < m ? ybar[r] : V(0);
+    const int len = (int)(pend - pbeg);
+    auto row_lane = [&](int q) {
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, rs, lo + step);
+        if (v <= q)
+          lo += step;
+      }
+      return lo;
+    };
+    int q0 = 0;
+    for (; q0 + 32 * U <= len; q0 += 32 * U) {
+      CI c[U];
+      V xv[U];
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        c[u] = __ldcs(colind + pbeg + q0 + lane + 32 * u);
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        xv[u] = ptx::ld_keep(x + c[u], pol_x);
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int q = q0 + lane + 32 * u;
+        const V yr = __shfl_sync(0xffffffffu, yb, row_lane(q));
+        __stcs(abar + pbeg + q, yr * xv[u]);
+      }
+    }
+    for (; q0 < len; q0 += 32) {
+      const int q = q0 + lane;
+      const bool in = q < len;
+      const CI c = in ? __ldcs(colind + pbeg + q) : CI(0);
+      const V xv = in ? ptx::ld_keep(x + c, pol_x) : V(0);
+      const V yr = __shfl_sync(0xffffffffu, yb, row_lane(q));
+      if (in)
+        __stcs(abar + pbeg + q, yr * xv);
+    }
+  }
+}
+
+template <class V, class CI, class RI>
+drb_status abar_rows_launch(Csr &A, const V *ybar, const V *x, V *abar, cudaStream_t s) {
+  static int grid_cache[64] = {0};
+  int &grid = grid_cache[A.device < 64 ? A.device : 0];
+  if (grid == 0) {
+    int occ = 0, sms = 0;
+    DRB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, abar_rows<V, CI, RI>, kAbRowsNT, 0));
+    DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
+    grid = std::max(1, occ) * sms;
+  }
+  const int64_t groups = (A.m + 31) / 32;
+  const int g = (int)std::max<int64_t>(
+      1, std::min<int64_t>(grid, (groups + kAbRowsNT / 32 - 1) / (kAbRowsNT / 32)));
+  abar_rows<V, CI, RI><<<g, kAbRowsNT, 0, s>>>(A.m, A.rowptr.as<RI>(), A.colind.as<CI>(),
+                                               ybar, x, abar);
+  note_launch();
+  DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
+}
+
+// Rows short enough for abar_rows (2048-entry 32-row groups at most, so a
+// static share of groups stays balanced).  Longer rows use the forward
+// product's work items (a 16.8M-row power-law matrix with rows up to 16384:
+// 1.73 ms on the items, 2.02 ms on 32-row groups).
+bool abar_short_rows(const Csr &A) { return A.max_row <= kAbRowsMaxLen; }
+
 template <class V, class CI, class RI, int TILE>
 drb_status abar_tile(Csr &A, const V *ybar, const V *x, V *abar, cudaStream_t s) {
   static int grid_cache[64] = {0};
@@ -344,6 +443,10 @@ drb_status abar_tile(Csr &A, const V *ybar, const V *x, V *abar, cudaStream_t s)
 template <class V, class CI, class RI>
 drb_status abar_typed(Csr &A, const V *ybar, const V *x, V *abar,
                       cudaStream_t s) {
+  if (A.nnz == 0)
+    return DRB_OK;
+  if (abar_short_rows(A))
+    return abar_rows_launch<V, CI, RI>(A, ybar, x, abar, s);
   if (A.pipe.nitems == 0)
     return DRB_OK;
   if (A.pipe.tile == 512)
@@ -421,10 +524,6 @@ drb_status spmv_t_launch(Csr &A, const void *ybar, void *xbar, cudaStream_t s) {
 
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
                        cudaStream_t s) {
-  // short regular rows: the sliced copy's lane-per-row layout (per-item row
-  // stamping costs more than the products on 5-nonzero rows)
-  if (A.sell.on && sell_abar_launch(A, ybar, x, abar, s) == DRB_OK)
-    return DRB_OK;
   if (A.storage == DRB_F32)
     return abar_v<float>(A, ybar, x, abar, s);
   if (A.storage == DRB_F64)

@@ -334,6 +334,8 @@ drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
   DRB_TRY(upload(A->vals.p, vb, values, vb_in, nnz, on_dev,
                  storage == DRB_BF16, s));
   DRB_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int64_t i = 0; i < m; i++)
+    A->max_row = std::max(A->max_row, rp_at(rp_h, ib, i + 1) - rp_at(rp_h, ib, i));
   DRB_TRY(build_plan(A->plan, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0, 0));
   DRB_TRY(build_pipe_plan(A->pipe, m, rp_h, ib, plan_group(vb, A->cbytes), 0, 0));
   DRB_TRY(sell_build(*A, rp_h, ib, s));

@@ -184,6 +184,7 @@ struct CgPlanDeleter {
 struct Csr {
   int device = 0;
   int64_t m = 0, n = 0, nnz = 0;
+  int64_t max_row = 0; // nonzeros in the longest row
   drb_dtype value_type = DRB_F32; // caller's element type
   drb_dtype storage = DRB_F32;    // device element type
   int cbytes = 4, rbytes = 4;     // stored index widths
@@ -191,7 +192,7 @@ struct Csr {
   drb_partition part = DRB_PART_ROW;
   uint32_t flags = 0;
   DevBuf rowptr, colind, vals;
-  Plan plan;      // row blocks: multi-RHS kernel and abar
+  Plan plan;      // row blocks: multi-RHS kernel
   PipePlan pipe;  // work items: the persistent single-RHS kernel
   Sell sell;      // sliced-ELL copy for short regular rows (when eligible)
   std::vector<int64_t> seg_row0, seg_row1, seg_nz0, seg_nz1;
@@ -238,10 +239,6 @@ drb_status pipe_check(Csr &A, cudaStream_t s);
 drb_status sell_build(Csr &A, const void *rowptr_host, int rbytes, cudaStream_t s);
 void sell_release(Csr &A);
 drb_status sell_pack_values(Csr &A, cudaStream_t s); // after the CSR values change
-// abar = ybar_i * x_j on the sliced copy (short regular rows); returns
-// DRB_ERR_UNSUPPORTED without launching when the copy is off or too wide.
-drb_status sell_abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
-                            cudaStream_t s);
 namespace warpk {
 struct WarpResid;
 }

@@ -204,62 +204,6 @@ __global__ void __launch_bounds__(kSellNT)
   }
 }
 
-// abar on the sliced copy: warp per slice, lane = row.  Lane r's k-th
-// product ybar[r] * x[col] lands in the warp's shared buffer at its CSR
-// offset from the slice's first nonzero, then the slice's contiguous CSR
-// range of abar is written with coalesced stores (writing abar directly
-// from the lanes would scatter every store over the slice's rows).
-constexpr int kSellAbWarps = 4;
-
-template <class V, class RI>
-__global__ void __launch_bounds__(kSellAbWarps * 32)
-    sell_abar(const int *__restrict__ cols, const int64_t *__restrict__ off, int64_t nslices,
-              int64_t m, const RI *__restrict__ rowptr, const V *__restrict__ ybar,
-              const V *__restrict__ x, V *__restrict__ abar, int maxw) {
-  extern __shared__ __align__(16) unsigned char sab_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  V *buf = reinterpret_cast<V *>(sab_raw) + (size_t)warp * 32 * maxw;
-  const int64_t w = (int64_t)blockIdx.x * kSellAbWarps + warp;
-  const int64_t W = (int64_t)gridDim.x * kSellAbWarps;
-  const int64_t a = nslices * w / W, b = nslices * (w + 1) / W;
-  const uint64_t pol_s = ptx::policy_evict_first();
-  const uint64_t pol_x = ptx::policy_evict_last();
-  for (int64_t sl = a; sl < b; sl++) {
-    const int64_t o = __ldg(off + sl);
-    const int wd = (int)((__ldg(off + sl + 1) - o) >> 5);
-    const int64_t r = sl * 32 + lane;
-    const int64_t rlast = min(sl * 32 + 32, m);
-    const int64_t base = (int64_t)rowptr[sl * 32];
-    const int64_t stop = (int64_t)rowptr[rlast];
-    int64_t rs = 0, len = 0;
-    V yb = V(0);
-    if (r < m) {
-      rs = (int64_t)rowptr[r] - base;
-      len = (int64_t)rowptr[r + 1] - base - rs;
-      yb = ybar[r];
-    }
-    // 8 column loads, then 8 gathers, then the products: all in flight at once
-    for (int k0 = 0; k0 < wd; k0 += 8) {
-      int c[8];
-#pragma unroll
-      for (int q = 0; q < 8; q++)
-        c[q] = k0 + q < wd ? ld_stream(cols + o + 32 * (k0 + q) + lane, pol_s) : 0;
-      V xv[8];
-#pragma unroll
-      for (int q = 0; q < 8; q++)
-        xv[q] = k0 + q < len ? warpk::ld_x(x + c[q], pol_x) : V(0);
-#pragma unroll
-      for (int q = 0; q < 8; q++)
-        if (k0 + q < len)
-          buf[rs + k0 + q] = yb * xv[q];
-    }
-    __syncwarp();
-    for (int64_t t = lane; t < stop - base; t += 32)
-      abar[base + t] = buf[t];
-    __syncwarp();
-  }
-}
-
 template <class V, bool RESID, int NS, int K> int sell_grid(int dev) {
   static int cache[64] = {0};
   int &g = cache[dev < 64 ? dev : 0];
@@ -394,42 +338,6 @@ drb_status sell_build(Csr &A, const void *rowptr_host, int rbytes, cudaStream_t 
   // used by default; DRB_SPMV_VARIANT naming a row-block variant keeps it off
   const char *e = std::getenv("DRB_SPMV_VARIANT");
   A.sell.on = !(e && std::strcmp(e, "sell") != 0);
-  return DRB_OK;
-}
-
-drb_status sell_abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
-                            cudaStream_t s) {
-  const Sell &S = A.sell;
-  const size_t vb = (size_t)dtype_bytes(A.storage);
-  const size_t smem = (size_t)kSellAbWarps * 32 * std::max(S.maxw, 1) * vb;
-  if (!S.on || S.nslices == 0 || smem > 48 * 1024)
-    return DRB_ERR_UNSUPPORTED; // the caller uses the work-item kernel
-  int sms = 0;
-  DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
-  const int64_t need = (S.nslices + kSellAbWarps - 1) / kSellAbWarps;
-  // 16 four-warp CTAs per SM: each warp's slices are a chain of dependent
-  // loads, so the latency is hidden by warps (8 per SM: FP64 Laplacian 0.100 ms)
-  const int g = (int)std::min<int64_t>((int64_t)sms * 16, need);
-  const bool r8 = A.rbytes == 8;
-#define DRB_SELL_ABAR(V, RI)                                                            \
-  sell_abar<V, RI><<<g, kSellAbWarps * 32, smem, s>>>(                                 \
-      S.cols.as<int>(), S.off.as<int64_t>(), S.nslices, A.m, A.rowptr.as<RI>(),           \
-      static_cast<const V *>(ybar), static_cast<const V *>(x), static_cast<V *>(abar),   \
-      S.maxw)
-  if (A.storage == DRB_F32) {
-    if (r8)
-      DRB_SELL_ABAR(float, int64_t);
-    else
-      DRB_SELL_ABAR(float, int32_t);
-  } else {
-    if (r8)
-      DRB_SELL_ABAR(double, int64_t);
-    else
-      DRB_SELL_ABAR(double, int32_t);
-  }
-#undef DRB_SELL_ABAR
-  note_launch();
-  DRB_CUDA_TRY(cudaGetLastError());
   return DRB_OK;
 }
 

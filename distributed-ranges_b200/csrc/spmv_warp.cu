@@ -157,9 +157,8 @@ drb_status fused_scratch(Csr &A) {
   PipePlan &P = A.pipe;
   int sms = 0;
   DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
-  // [per-CTA partials][split-row terms][ticket, 16 bytes][per-item partials]
-  const size_t bytes =
-      sizeof(double) * ((size_t)sms * 32 + (size_t)P.nsplit + (size_t)P.nitems) + 16;
+  // [per-CTA partials][ticket, 16 bytes][per-item partials]
+  const size_t bytes = sizeof(double) * ((size_t)sms * 32 + (size_t)P.nitems) + 16;
   if (!P.red.p || P.red.bytes < bytes) {
     DRB_TRY(P.red.alloc(bytes));
     DRB_CUDA_TRY(cudaMemset(P.red.p, 0, P.red.bytes));
@@ -178,13 +177,11 @@ drb_status fused_pipe_launch(Csr &A, const void *x, const void *b, void *y, doub
   }
   int sms = 0;
   DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
-  const size_t slots = (size_t)sms * 32 + (size_t)P.nsplit;
+  const size_t slots = (size_t)sms * 32;
   DRB_TRY(fused_scratch(A));
   WarpResid ra;
   ra.b = b;
   ra.partials = P.red.as<double>();
-  ra.rowres = P.red.as<double>() + (size_t)sms * 32;
-  ra.nsplit = P.nsplit;
   ra.ticket = reinterpret_cast<int *>(P.red.as<double>() + slots);
   ra.ipart = P.red.as<double>() + slots + 2;
   ra.out = out;

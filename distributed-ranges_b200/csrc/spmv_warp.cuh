@@ -134,10 +134,10 @@ __device__ __forceinline__ int skew(int q) { return q + (q >> 5); }
 
 // Fused row reduction: ||A x - b||^2, or with `dot` set sum_i y_i b_i (b is
 // then a weight vector, e.g. p for p.Ap).  The whole rows of work item i add
-// into their own slot ipart[i] (whichever warp ran the item); a chunked row's
-// term goes to its own slot rowres[counter], written by the finish pass.  The
-// finish pass's CTAs sum fixed ranges of ipart into partials[cta] and its
-// last CTA sums partials[0..grid) then rowres[0..nsplit) in order, so the
+// into their own slot ipart[i] (whichever warp ran the item).  The finish
+// pass completes the chunked rows; its CTA c adds the terms of the split rows
+// it completes (a fixed grid-stride share) and a fixed range of ipart into
+// partials[c], and its last CTA sums partials[0..grid) in order, so the
 // result never depends on the schedule.  (The sliced-ELL kernel writes one
 // partial per CTA and combines them itself.)  A non-null `stop` pointing at
 // a non-zero word makes the launches return before touching anything (a
@@ -146,8 +146,6 @@ struct WarpResid {
   const void *b = nullptr;
   double *partials = nullptr;
   double *ipart = nullptr;
-  double *rowres = nullptr;
-  int64_t nsplit = 0;
   int *ticket = nullptr;
   double *out = nullptr;
   const int *stop = nullptr;
@@ -232,8 +230,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
   // Runs the item in `sl` and refills the slot with item `refill`.
   template <bool RESID>
   __device__ __forceinline__ void process(S &sl, int64_t refill, Acc *prod, int *srp,
-                                          const Acc *bvec, double &r2, double *rowres,
-                                          bool dotw) {
+                                          const Acc *bvec, double &r2, bool dotw) {
     const Item cur = sl.d;
     const int off = (int)(cur.p0 - sl.a0), end = off + cur.len;
     const int ng = (end + G - 1) / G;
@@ -268,7 +265,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       fetch(sl, refill);
       const Acc tot = group_sum(acc.s, acc.c, 32);
       if (lane == 0)
-        finish_chunk<RESID>(cur, tot, bvec, rowres, dotw);
+        partials[cur.chunk] = tot; // the row is completed by the finish pass
       return;
     }
 #pragma unroll
@@ -335,13 +332,6 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     __syncwarp(); // the shared slice is rewritten by the next item
   }
 
-  // Lane 0 after a chunk: publish the partial.  The split row is completed
-  // by a second pass (chunk_finish / resid_finish) in chunk order.
-  template <bool RESID>
-  __device__ __forceinline__ void finish_chunk(const Item &cur, Acc tot, const Acc *,
-                                               double *, bool) {
-    partials[cur.chunk] = tot;
-  }
 };
 
 template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP>
@@ -395,7 +385,7 @@ __global__ void __launch_bounds__(kThreads)
   K.fetch(A, cur);
   int64_t next = advance();
   while (A.valid) {
-    K.template process<RESID>(A, next, prod, srp, bvec, r2, ra.rowres, ra.dot != 0);
+    K.template process<RESID>(A, next, prod, srp, bvec, r2, ra.dot != 0);
     if (RESID) {
       // the item's whole rows, in row order within each lane, then a fixed tree
       const double t = wsum(r2);
@@ -430,10 +420,11 @@ __global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64
   }
 }
 
-// The fused row reduction's second pass: split rows as in chunk_finish, each
-// also adding its term to rowres[counter]; CTA b sums the item slots
-// ipart[b * per, (b + 1) * per) into partials[b]; the last CTA (ticket) then
-// adds partials[0..grid) and rowres[0..nsplit) in index order into *out.
+// The fused row reduction's second pass: split rows as in chunk_finish; CTA
+// c adds the terms of the split rows it completes (chunks c * kThreads + t,
+// strided by the grid) and the item slots ipart[c * per, (c + 1) * per) into
+// partials[c]; the last CTA (ticket) adds partials[0..grid) in index order
+// into *out.  The grid is a function of the plan, so the grouping is fixed.
 // Returns at once when the stop word is set.
 template <class Acc, bool COMP>
 __global__ void __launch_bounds__(kThreads)
@@ -446,43 +437,49 @@ __global__ void __launch_bounds__(kThreads)
     return;
   const Acc *bvec = static_cast<const Acc *>(ra.b);
   const int64_t nth = (int64_t)gridDim.x * kThreads;
+  double sum = 0.0;
   for (int64_t c = (int64_t)blockIdx.x * kThreads + threadIdx.x; c < nchunks; c += nth) {
     const Chunk ch = chunks[c];
     if (ch.first != c)
       continue;
-    CSum<Acc> sum;
+    CSum<Acc> rs;
     for (int i = 0; i < ch.count; i++) {
       const Acc p = cpart[ch.first + i];
       if (COMP)
-        sum.add(p);
+        rs.add(p);
       else
-        sum.s += p;
+        rs.s += p;
     }
-    const Acc v = sum.value();
+    const Acc v = rs.value();
     y[ch.row] = v;
     const double dd = (double)v - (double)bvec[ch.row];
-    ra.rowres[ch.counter] = ra.dot ? (double)v * (double)bvec[ch.row] : dd * dd;
+    sum += ra.dot ? (double)v * (double)bvec[ch.row] : dd * dd;
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   {
     const int64_t per = (nitems + gridDim.x - 1) / gridDim.x;
     const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(nitems, i0 + per);
-    double sum = 0.0;
-    for (int64_t i = i0 + threadIdx.x; i < i1; i += kThreads)
-      sum += ra.ipart[i];
-    sum = wsum(sum);
-    if (lane == 0)
-      s_red[warp] = sum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double cta = 0.0;
-      for (int w = 0; w < kWarps; w++)
-        cta += s_red[w];
-      ra.partials[blockIdx.x] = cta;
+    int64_t i = i0 + threadIdx.x;
+    for (; i + 3 * kThreads < i1; i += 4 * kThreads) { // four loads in flight
+      const double a0 = ra.ipart[i], a1 = ra.ipart[i + kThreads];
+      const double a2 = ra.ipart[i + 2 * kThreads], a3 = ra.ipart[i + 3 * kThreads];
+      sum += a0;
+      sum += a1;
+      sum += a2;
+      sum += a3;
     }
+    for (; i < i1; i += kThreads)
+      sum += ra.ipart[i];
   }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  sum = wsum(sum);
+  if (lane == 0)
+    s_red[warp] = sum;
   __syncthreads();
   if (threadIdx.x == 0) {
+    double cta = 0.0;
+    for (int w = 0; w < kWarps; w++)
+      cta += s_red[w];
+    ra.partials[blockIdx.x] = cta;
     __threadfence();
     s_last = atomicAdd(ra.ticket, 1) == (int)gridDim.x - 1;
   }
@@ -490,14 +487,13 @@ __global__ void __launch_bounds__(kThreads)
   if (!s_last)
     return;
   __threadfence();
-  const int64_t np = gridDim.x, total = np + ra.nsplit;
-  double sum = 0.0;
-  for (int64_t i = threadIdx.x; i < total; i += kThreads)
-    sum += i < np ? __ldcg(&ra.partials[i]) : __ldcg(&ra.rowres[i - np]);
-  sum = wsum(sum);
+  double t = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads)
+    t += __ldcg(&ra.partials[i]);
+  t = wsum(t);
   __syncthreads(); // s_red is reused
   if (lane == 0)
-    s_red[warp] = sum;
+    s_red[warp] = t;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t2 = 0.0;

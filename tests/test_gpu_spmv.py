@@ -491,6 +491,32 @@ def test_adjoint_against_transposed_oracle(mp, dtype, kind):
     assert rel_err(xbar.cpu().numpy(), 2 * xb_ref, 2 * d) <= tol
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("m", [1, 31, 33, 1031])
+def test_abar_short_rows_edges(mp, dtype, m):
+    """Rows of 0..64 nonzeros (many empty, m not a multiple of the 32-row
+    groups): abar = ybar_i * x_j is one rounded product per entry, so it
+    matches numpy's bit for bit."""
+    rng = np.random.default_rng(m)
+    n = 700
+    lens = rng.integers(0, 65, m)
+    lens[rng.random(m) < 0.3] = 0
+    lens[0] = 64
+    rp = np.zeros(m + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in lens]
+                        + [np.zeros(0, np.int64)]).astype(np.int32)
+    v = rng.uniform(-1, 1, len(ci)).astype(dtype)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    yb = rng.uniform(-1, 1, m).astype(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0, adjoint=True)
+    tdt = torch.from_numpy(x).dtype
+    abar = torch.full((len(v),), 7.0, dtype=tdt, device="cuda")
+    mp.gemv_backward(a, torch.from_numpy(yb).cuda(), torch.from_numpy(x).cuda(), None, abar)
+    rows = np.repeat(np.arange(m), lens)
+    assert np.array_equal(abar.cpu().numpy(), yb[rows] * x[ci])
+
+
 def test_adjoint_finite_differences_laplacian(mp):
     """Central differences (h = 1e-6, fp64) of L = 0.5 ||A x - b||^2 through
     the forward gemv.  The loss difference is formed row by row as
