@@ -10,9 +10,9 @@
 // "long row").  An item is 16 bytes {matrix, first row, rows | nnz << 8,
 // first nonzero}; the items of all matrices form one list, and with more
 // right-hand sides than one block holds, (item, block) pairs are the units.
-// Warp w of the persistent grid runs units w, w + W, w + 2W, ... (W = warps in
-// the grid): units hold at most CAP nonzeros, so the static split balances,
-// and no warp waits on another (no spin anywhere).
+// Warps of the persistent grid take units in batches of 8 consecutive indices
+// from a work counter (zeroed by a memset node before the kernel in the
+// graph); no warp waits on another (no spin anywhere).
 //
 // Random gathers of X rows bound this kernel.  Every warp runs a software
 // pipeline over its units: while unit t computes, the column indices,
@@ -78,6 +78,7 @@ struct BArgs {
   int warp_bytes;
   int cols_off, cols_stage, vals_off, vals_stage, rs_off, rs_stage;
   int y_off;
+  unsigned long long *counter; // next unit to take (zeroed before each launch)
 };
 
 template <class V> struct AccOf {
@@ -239,18 +240,35 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
   const bool on = slot < S;
   const bool row_on = on && grp < R; // slots past R*G idle in short units
   const int ystride = KB + 1;
-  const int64_t W = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t nunits = a.nunits;
   const int nkb = a.nkb;
   constexpr int VOFF_MASK = 16 / (int)sizeof(V) - 1;
 
-  int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  // the warp's units: batches of kGrab consecutive units from the work
+  // counter, so the sequence only grows, and which warp runs a unit never
+  // changes its rows' sums.  (A static split -- warp w taking units w, w + W,
+  // ... -- left warps idle behind unlucky shares: the 512-matrix batch ran
+  // 22-26 ms on its best variant, varying run to run; batched grabs: 17.5 ms.)
+  constexpr int kGrab = 8;
+  int64_t gbase = 0;
+  int gk = kGrab;
+  auto next_unit = [&]() -> int64_t {
+    if (gk == kGrab) {
+      unsigned long long v = 0;
+      if (lane == 0)
+        v = atomicAdd(a.counter, (unsigned long long)kGrab);
+      gbase = (int64_t)__shfl_sync(0xffffffffu, v, 0);
+      gk = 0;
+    }
+    return gbase + gk++;
+  };
   auto item_of = [&](int64_t uu) -> int64_t {
     return nkb == 1 ? uu : (int64_t)((uint32_t)uu / (uint32_t)nkb);
   };
+  int64_t u = next_unit();
+  int64_t u1 = next_unit();
   int4 rec = u < nunits ? __ldg(a.items + item_of(u)) : make_int4(0, 0, 0, 0);
-  int4 rec_n = u + W < nunits ? __ldg(a.items + item_of(u + W))
-                              : make_int4(0, 0, 0, 0);
+  int4 rec_n = u1 < nunits ? __ldg(a.items + item_of(u1)) : make_int4(0, 0, 0, 0);
 
   // slices (columns, values, row offsets) of a short unit -> stage st
 #define DRB_BATCH_PAIRS(REC, VALID, ST)                                          \
@@ -269,10 +287,10 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
   } while (0)
 
   DRB_BATCH_PAIRS(rec, u < nunits, 0);
-  for (int st = 0; u < nunits; u += W, st ^= 1) {
-    const int4 rec_nn = u + 2 * W < nunits ? __ldg(a.items + item_of(u + 2 * W))
-                                           : make_int4(0, 0, 0, 0);
-    DRB_BATCH_PAIRS(rec_n, u + W < nunits, st ^ 1);
+  for (int st = 0; u < nunits; st ^= 1) {
+    const int64_t u2 = next_unit();
+    const int4 rec_nn = u2 < nunits ? __ldg(a.items + item_of(u2)) : make_int4(0, 0, 0, 0);
+    DRB_BATCH_PAIRS(rec_n, u1 < nunits, st ^ 1);
     cp_wait<1>(); // all but the newest group: the slices of unit u
     __syncwarp();
 
@@ -380,6 +398,8 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
     }
     rec = rec_n;
     rec_n = rec_nn;
+    u = u1;
+    u1 = u2;
   }
 #undef DRB_BATCH_PAIRS
   cp_wait<0>();
@@ -527,7 +547,7 @@ struct Batch {
   std::vector<Csr *> mats;
   std::vector<BMat> hmats;
   std::vector<PackEnt> hpack;
-  DevBuf dmats, items, xpack, dpack;
+  DevBuf dmats, items, xpack, dpack, counter;
   bool bound = false;
   bool use_graph = true;
   cudaGraph_t graph = nullptr;
@@ -627,6 +647,9 @@ drb_status configure(Batch &B, int G) {
   B.grid = (int)std::max<int64_t>(
       1, std::min<int64_t>((int64_t)per_sm * sms, want));
   a.nunits = units;
+  if (!B.counter.p)
+    DRB_TRY(B.counter.alloc(16));
+  a.counter = B.counter.as<unsigned long long>();
   a.nkb = B.nkb;
   a.k = (int)B.k;
   a.ldx = B.ldx;
@@ -689,6 +712,7 @@ drb_status enqueue(Batch &B, cudaStream_t s, bool count) {
     n++;
   }
   if (B.args.nunits > 0) {
+    DRB_CUDA_TRY(cudaMemsetAsync(B.args.counter, 0, sizeof(unsigned long long), s));
     B.kernel<<<B.grid, B.warps * 32, (size_t)B.warps * B.args.warp_bytes, s>>>(
         B.args);
     DRB_CUDA_TRY(cudaGetLastError());

@@ -374,7 +374,7 @@ def test_dense_gemv(mp, dtype, m, n, k, pad, layout):
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-@pytest.mark.parametrize("n", [0, 1, 7, 1000, 1 << 20, (1 << 20) + 3])
+@pytest.mark.parametrize("n", [0, 1, 7, 1000, 1 << 20, (1 << 20) + 3, 5_000_011])
 def test_dot(mp, dtype, n):
     g = torch.Generator().manual_seed(n)
     a = torch.randn(n, generator=g, dtype=torch.float64).to(dtype)
@@ -385,6 +385,10 @@ def test_dot(mp, dtype, n):
     got = float(out.item())
     assert got == float(out2.item())        # deterministic
     assert abs(got - ref) <= 1e-12 * max(1.0, float((a.double().abs() * b.double().abs()).sum()))
+    if n:
+        ad = a.cuda()
+        nrm = float(mp.dot(ad, ad).item())   # a is b: one stream read
+        assert abs(nrm - oracle.dot(a.numpy(), a.numpy())) <= 1e-12 * nrm
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
