@@ -767,7 +767,7 @@ drb_status launch(Batch &B, cudaStream_t s) {
   return enqueue(B, s, true);
 }
 
-drb_status make_batch(Batch &B, int32_t count, const drb_csr_t *handles,
+drb_status make_batch(Batch &B, int32_t count, Csr *const *handles,
                       int64_t k, drb_layout layout, uint32_t flags) {
   if (count < 1)
     return fail(DRB_ERR_INVALID_ARG, "invalid argument: count < 1");
@@ -997,9 +997,53 @@ drb_status autotune(Batch &B, cudaStream_t s, int *chosen) {
 } // namespace
 } // namespace drb
 
+namespace drb {
+
+void BatchDeleter::operator()(Batch *p) const { delete p; }
+
+drb_status multi_rhs_batch_launch(Csr &A, const void *x, void *y, int64_t k,
+                                  drb_layout layout, cudaStream_t s, bool *used) {
+  *used = false;
+  if (A.cbytes != 4 || A.rbytes != 4 || A.nnz == 0 || A.m >= ((int64_t)1 << 31) ||
+      (layout == DRB_ROW_MAJOR && reinterpret_cast<uintptr_t>(x) % 16 != 0))
+    return DRB_OK;
+  if (!A.mrhs || A.mrhs_k != k || A.mrhs_layout != (int)layout) {
+    A.mrhs.reset();
+    std::unique_ptr<Batch, BatchDeleter> B(new Batch());
+    Csr *one = &A;
+    DRB_TRY(make_batch(*B, 1, &one, k, layout, A.flags & DRB_FLAG_BF16_X_F32));
+    DRB_CUDA_TRY(cudaStreamSynchronize(s)); // the work list is built on the host
+    DRB_TRY(capture(*B));
+    if (A.flags & DRB_FLAG_AUTOTUNE) {
+      // times the variants writing y = A X (x is only read), then keeps one
+      DRB_TRY(bind(*B, &x, &y, s));
+      DRB_TRY(autotune(*B, s, nullptr));
+    }
+    A.mrhs = std::move(B);
+    A.mrhs_k = k;
+    A.mrhs_layout = (int)layout;
+  }
+  DRB_TRY(bind(*A.mrhs, &x, &y, s));
+  DRB_TRY(launch(*A.mrhs, s));
+  *used = true;
+  return DRB_OK;
+}
+
+} // namespace drb
+
 using namespace drb;
 
 struct drb_batch_plan : public Batch {};
+
+namespace {
+// The handles as the library's matrix type (NULL stays NULL).
+std::vector<Csr *> as_mats(int32_t count, const drb_csr_t *handles) {
+  std::vector<Csr *> v;
+  if (handles && count > 0)
+    v.assign(handles, handles + count);
+  return v;
+}
+} // namespace
 
 extern "C" {
 
@@ -1010,13 +1054,15 @@ drb_status drb_batch_create(drb_batch_t *out, int32_t count,
   if (!out)
     return fail(DRB_ERR_INVALID_ARG, "invalid argument: out is NULL");
   *out = nullptr;
+  const std::vector<Csr *> mats = as_mats(count, handles);
+  Csr *const *hs = handles ? mats.data() : nullptr;
   if (count < 1 || !handles || !handles[0]) {
     Batch probe;
-    return make_batch(probe, count, handles, k, layout, flags);
+    return make_batch(probe, count, hs, k, layout, flags);
   }
   DeviceGuard g(handles[0]->device);
   auto P = std::make_unique<drb_batch_plan>();
-  DRB_TRY(make_batch(*P, count, handles, k, layout, flags));
+  DRB_TRY(make_batch(*P, count, hs, k, layout, flags));
   DRB_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
   DRB_TRY(capture(*P));
   *out = P.release();
@@ -1081,12 +1127,14 @@ drb_status drb_batched_gemv(int32_t count, const drb_csr_t *handles,
                             drb_layout layout, uint32_t flags, void *stream) {
   clear_error();
   Batch probe;
+  const std::vector<Csr *> mats = as_mats(count, handles);
+  Csr *const *hs = handles ? mats.data() : nullptr;
   if (count < 1 || !handles || !handles[0])
-    return make_batch(probe, count, handles, k, layout, flags);
+    return make_batch(probe, count, hs, k, layout, flags);
   DeviceGuard g(handles[0]->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   probe.use_graph = false;
-  DRB_TRY(make_batch(probe, count, handles, k, layout, flags));
+  DRB_TRY(make_batch(probe, count, hs, k, layout, flags));
   DRB_TRY(bind(probe, x, y, s));
   DRB_TRY(launch(probe, s));
   DRB_CUDA_TRY(cudaStreamSynchronize(s));

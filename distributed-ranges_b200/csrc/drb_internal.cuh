@@ -180,6 +180,10 @@ struct CgPlan; // conjugate-gradient workspace (cg.cu)
 struct CgPlanDeleter {
   void operator()(CgPlan *p) const;
 };
+struct Batch; // batched SpMM plan (batch.cu)
+struct BatchDeleter {
+  void operator()(Batch *p) const;
+};
 
 struct Csr {
   int device = 0;
@@ -210,12 +214,21 @@ struct Csr {
   std::vector<cudaEvent_t> seg_done;
   // conjugate-gradient workspace and its captured iteration graph
   std::unique_ptr<CgPlan, CgPlanDeleter> cg;
+  // k > 1 products: a batch of this one handle, for one (k, layout)
+  std::unique_ptr<Batch, BatchDeleter> mrhs;
+  int64_t mrhs_k = 0;
+  int mrhs_layout = -1;
   // host copy of rowptr (int64), filled on first drb_csr_get_entries
   std::vector<int64_t> rowptr_h;
   ~Csr();
 };
 
 // ---- launchers (defined in the .cu files) ------------------------------------
+// y = A X for k > 1 through a cached batch of this one handle (batch.cu);
+// *used = false, without launching, when the handle or the call does not
+// qualify (64-bit indices, no nonzeros, misaligned row-major X).
+drb_status multi_rhs_batch_launch(Csr &A, const void *x, void *y, int64_t k,
+                                  drb_layout layout, cudaStream_t s, bool *used);
 drb_status build_plan(Plan &plan, int64_t m, const void *rowptr_host,
                       int rbytes, int group, int tile, int rows_max,
                       int long_max);

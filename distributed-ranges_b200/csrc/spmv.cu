@@ -6,8 +6,10 @@
 // and csr_eq_distribution::local_gemv (csr_eq_distribution.hpp:54-131): all
 // segments of the matrix are resident on one GPU and one launch covers them.
 // One right-hand side (k = 1) and the fused residual run the persistent warp
-// kernel (spmv_warp.cu); k > 1 runs spmm_rowblocks below over CTA work items
-// ("row blocks", built once per matrix):
+// kernel (spmv_warp.cu); k > 1 runs the batched SpMM kernel on a batch of the
+// one handle (batch.cu), or, for what a batch does not take (64-bit indices,
+// misaligned row-major X), spmm_rowblocks below over CTA work items ("row
+// blocks", built once per matrix):
 //   * rows   : consecutive short rows, one warp per row;
 //   * long   : one row longer than a tile: the whole CTA loops over it;
 //   * chunk  : a row longer than long_max is split into chunks; each CTA
@@ -289,13 +291,21 @@ drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
                        drb_layout layout, cudaStream_t s) {
   if (k == 1)
     return spmv_pipe_launch(A, x, y, s);
+  // k > 1: the batched SpMM kernel on a batch of this one handle (2.0-2.3x
+  // the row-block kernel below at k = 2..20 on 4M-row and 16.8M-row
+  // matrices); the row-block kernel covers what a batch does not take
+  bool used = false;
+  DRB_TRY(multi_rhs_batch_launch(A, x, y, k, layout, s, &used));
+  if (used)
+    return DRB_OK;
   switch (A.storage) {
   case DRB_F32:
     return dispatch_idx<float>(A, x, y, k, layout, s);
   case DRB_F64:
     return dispatch_idx<double>(A, x, y, k, layout, s);
   default:
-    set_error("multi-RHS gemv takes F32 or F64 storage (BF16: k = 1, or drb_batch_*)");
+    set_error("multi-RHS gemv with 64-bit indices or a misaligned row-major x takes F32 or "
+              "F64 storage");
     return DRB_ERR_UNSUPPORTED;
   }
 }

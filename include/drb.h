@@ -142,8 +142,13 @@ drb_status drb_csr_get_entries(drb_csr_t A, int64_t offset, int64_t count,
 
 /* y = A * x for k right-hand sides, device pointers.  Element types: x and y
  * have the storage type, except BF16 storage: x bf16 (f32 with
- * DRB_FLAG_BF16_X_F32), y f32, products exact in f32 and summed with two-sum
- * compensation.  BF16 storage takes k = 1.  y is overwritten (the reference
+ * DRB_FLAG_BF16_X_F32), y f32, products exact in f32 (k = 1: summed with
+ * two-sum compensation; k > 1: plain f32 sums, as drb_batch_*).  k > 1 runs
+ * the batched SpMM kernel on a batch of this one handle, built on the first
+ * call with a given (k, layout) -- that call synchronises `stream`, and the
+ * handle then keeps a row-major copy of X (n * k elements, rows padded to 16
+ * bytes) -- or, for 64-bit indices or a row-major x not 16-byte aligned, a
+ * row-block kernel (F32/F64 only).  y is overwritten (the reference
  * zero-fills its partial result first). */
 drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
                         drb_layout layout, void *stream);

@@ -262,6 +262,63 @@ def test_multi_rhs(mp, k, layout, dtype):
     assert rel_err(Y.ravel(), y64.ravel(), d.ravel()) <= tol
 
 
+@pytest.mark.parametrize("layout", [0, 1])
+def test_multi_rhs_fallback_and_repeat(mp, layout):
+    """k > 1 runs on a batch of the one handle; 64-bit indices (kept) and a
+    row-major x off a 16-byte boundary take the row-block kernel instead.
+    Both agree with the oracle, and repeated calls (the cached batch, and a
+    new k that rebuilds it) give the same bits."""
+    rp, ci, v, m, n = chunky_matrix(np.float64, np.int64)
+    k = 5
+    rng = np.random.default_rng(9)
+    X = rng.uniform(-1, 1, (n, k))
+    xin = X.T.ravel() if layout == 0 else X.ravel()
+    y64 = oracle.gemv_row(rp, ci, v, X.T.ravel(), m, n, k, oracle.ACC_LD).reshape(k, m).T
+    d = oracle.absdot(rp, ci, v, X.T.ravel(), m, n, k).reshape(k, m).T
+    outs = []
+    for keep64 in (False, True):
+        a, y = gpu_gemv(mp, rp, ci, v, m, n, xin, k, layout, keep_index64=keep64)
+        Y = y.reshape(k, m).T if layout == 0 else y.reshape(m, k)
+        assert rel_err(Y.ravel(), y64.ravel(), d.ravel()) <= 1e-12
+        outs.append(y)
+        if not keep64:
+            xt = torch.from_numpy(xin).cuda()
+            y2 = torch.empty(m * k, dtype=torch.float64, device="cuda")
+            a.gemv_device(xt, y2, k, layout)
+            a.gemv_device(torch.zeros(n * 3, dtype=torch.float64, device="cuda"),
+                          torch.empty(m * 3, dtype=torch.float64, device="cuda"), 3, layout)
+            a.gemv_device(xt, y2, k, layout)
+            assert np.array_equal(y2.cpu().numpy(), y)
+    if layout == 1:
+        # a row-major x at an 8-byte offset: the row-block kernel
+        a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+        buf = torch.from_numpy(np.concatenate([[0.0], xin])).cuda()
+        y3 = torch.empty(m * k, dtype=torch.float64, device="cuda")
+        a.gemv_device(buf[1:], y3, k, layout)
+        Y = y3.cpu().numpy().reshape(m, k)
+        assert rel_err(Y.ravel(), y64.ravel(), d.ravel()) <= 1e-12
+
+
+def test_multi_rhs_bf16(mp):
+    """BF16 storage with k > 1 (the batched kernel's plain f32 sums): within
+    f32 accumulation error of the FP64 product of the bf16-rounded inputs."""
+    import drb
+    m = 20_000
+    rp, ci, v = drb.gen.uniform_rows_csr(m, m, lo=1, hi=90, seed=4)
+    k = 6
+    X = np.random.default_rng(5).uniform(-1, 1, (m, k)).astype(np.float32)
+    xb = torch.from_numpy(X.T.ravel().copy()).to(torch.bfloat16)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, m)), 0,
+                                     storage=torch.bfloat16)
+    y = torch.empty(m * k, dtype=torch.float32, device="cuda")
+    a.gemv_device(xb.cuda(), y, k, 0)
+    vr = torch.from_numpy(v).to(torch.bfloat16).double().numpy()
+    xr = xb.double().numpy()
+    ref = oracle.gemv_row(rp, ci, vr, xr, m, m, k, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, vr, xr, m, m, k)
+    assert rel_err(y.cpu().numpy(), ref, d) <= 1e-5
+
+
 def test_host_gemv_matches_device(mp):
     import drb
     m = 50_000
