@@ -79,30 +79,71 @@ def profiled_traffic(name):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: through NVML every 2 ms (reads only), else nvidia-smi every 0.1 s.
+    The GPU is matched to the CUDA device by UUID."""
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.samples = []
+        self.samples = []  # (sm_mhz, max_mhz, set of active reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                uuid = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            bits = [pynvml.nvmlClocksEventReasonHwSlowdown,
+                    pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    pynvml.nvmlClocksEventReasonSwPowerCap]
+            self._nvml = (pynvml, h, bits)
+            self._nvml_sample()
+        except Exception:
+            self._nvml = None
+            self.samples = []
+
+    def _nvml_sample(self):
+        nv, h, bits = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((float(sm), float(mx),
+                             {n for n, b in zip(self.NAMES, bits) if r & b}))
+
+    def _smi_sample(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                              "--format=csv,noheader,nounits"], capture_output=True,
+                             text=True, timeout=5).stdout.strip()
+        f = [t.strip() for t in out.split(",")] if out else []
+        if len(f) >= 2 and f[0].replace(".", "").isdigit():
+            self.samples.append((float(f[0]), float(f[1]) if f[1].replace(".", "").isdigit()
+                                 else float("nan"),
+                                 {self.NAMES[i] for i in range(4)
+                                  if len(f) > 2 + i and f[2 + i].lower().startswith("active")}))
 
     def _run(self):
+        period = 0.002 if self._nvml else 0.1
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                      "--format=csv,noheader,nounits"], capture_output=True,
-                                     text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([s.strip() for s in out.split(",")])
+                self._nvml_sample() if self._nvml else self._smi_sample()
             except Exception:
                 return
-            self._stop.wait(0.1)
+            self._stop.wait(period)
 
     def __enter__(self):
+        self.samples = []
+        self.source = "nvml" if self._nvml else "nvidia-smi"
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
         return self
@@ -115,14 +156,12 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4)
-                          if len(s) > 2 + i and s[2 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
+        sm = [s[0] for s in self.samples]
+        mx = [s[1] for s in self.samples if s[1] == s[1]]
+        reasons = sorted(set().union(*[s[2] for s in self.samples]))
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm),
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(self.samples), "source": self.source}
 
 
 def make_workload(nthreads=0):
@@ -381,6 +420,20 @@ def extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes32, fwd_ms, stream):
     ms = statistics.mean(timed_launches(lambda: mp.residual_norm2(A, xd, b, yd), steps, stream))
     rb = bytes32 + 4 * M
     out["residual_fused"] = {"ms": round(ms, 4), "GBps": round(rb / (ms * 1e-3) / 1e9, 2)}
+
+    # k = 16 right-hand sides on the same matrix (column-major X and Y, the
+    # broadcasted_slim_matrix layout): the batched kernel on this one handle
+    k16 = 16
+    X16 = torch.empty(N_COLS * k16, device="cuda").uniform_(-1, 1)
+    Y16 = torch.empty(M * k16, device="cuda")
+    A.gemv_device(X16, Y16, k16)  # first call: builds the handle's batch
+    ms = statistics.mean(timed_launches(lambda: A.gemv_device(X16, Y16, k16), steps, stream))
+    b16 = alg_bytes(M, N_COLS, nnz, 4, 4, 4, 4, 4, k16)
+    out["spmm_k16"] = {"ms": round(ms, 4), "GBps": round(b16 / (ms * 1e-3) / 1e9, 2),
+                       "frac": round(b16 / (ms * 1e-3) / 1e9 / peak, 4),
+                       "gflops": round(2 * nnz * k16 / (ms * 1e-3) / 1e9, 2),
+                       "vs_16_spmvs": round(16 * fwd_ms / ms, 2)}
+    del X16, Y16
 
     # FP64 SpMV on the same pattern
     A64 = mp.distributed_sparse_matrix(mp.csr_matrix_view(v.astype(np.float64), rp, ci,
