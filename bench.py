@@ -1002,6 +1002,8 @@ def profile_case(name):
                product layout) on the first 4,194,304 rows' worth of the bench
                distribution (16,777,216 columns, so the same 64 MB x);
       residual4m  the fused ||Ax - b||^2 on that matrix (same variant);
+      adjoint_lap_f32  gemv_backward (xbar and abar) on the 2048^2 5-point
+               Laplacian, FP32, random values;
       dot_f32  the dot kernel on two FP32 vectors of 2^26 elements (2 x 256 MB)."""
     import torch
     import drb
@@ -1087,6 +1089,20 @@ def profile_case(name):
             else:
                 mp.residual_norm2(A, x, b, y)
         A.check()
+    elif name == "adjoint_lap_f32":
+        rp, ci, v = drb.gen.laplacian2d_csr(2048, value_dtype=np.float32)
+        m = len(rp) - 1
+        v = np.random.default_rng(SEED + 13).uniform(-1, 1, len(v)).astype(np.float32)
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp.astype(np.int32), ci, (m, m)),
+                                         0, distr=mp.csr_row_distribution, adjoint=True)
+        g = torch.Generator(device="cuda").manual_seed(SEED + 14)
+        x = torch.randn(m, device="cuda", generator=g)
+        yb = torch.randn(m, device="cuda", generator=g)
+        xbar = torch.empty(m, device="cuda")
+        abar = torch.empty(len(v), device="cuda")
+        for _ in range(4):
+            mp.gemv_backward(A, yb, x, xbar, abar)
+        A.check()
     elif name == "dot_f32":
         g = torch.Generator(device="cuda").manual_seed(SEED + 12)
         a = torch.empty(1 << 26, device="cuda").uniform_(-1, 1, generator=g)
@@ -1116,7 +1132,8 @@ def main():
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
     ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64",
-                                               "cg_f64", "powerlaw4m", "residual4m", "dot_f32"],
+                                               "cg_f64", "powerlaw4m", "residual4m", "dot_f32",
+                                               "adjoint_lap_f32"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
