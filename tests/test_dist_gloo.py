@@ -1,5 +1,5 @@
-"""Multi-process gemv (drb.dist) on CPU ranks over gloo: world sizes 2 and
-3, csr_row and csr_eq, root and no-root forms, a 20-wide slim matrix,
+"""Multi-process gemv (drb.dist) on CPU ranks over gloo: world sizes 2, 3
+and 4, csr_row and csr_eq, root and no-root forms, a 20-wide slim matrix,
 segments and iteration -- each rank's product is the oracle's loop, so the
 assembled results must equal the oracle's restatement of the reference's
 per-rank loops and gather bit for bit (see tests/dist_rank.py)."""
@@ -41,7 +41,7 @@ def run_ranks(world: int, local: str, backend: str, timeout: int = 300):
     return outs
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_sharded_gemv_gloo_matches_oracle_bitwise(world):
     outs = run_ranks(world, "oracle", "gloo")
     for rc, out in outs:
