@@ -164,12 +164,17 @@ class ClockSampler:
                 "samples": len(self.samples), "source": self.source}
 
 
-def make_workload(nthreads=0):
-    import drb
-    alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
-    rp, ci, v = drb.gen.powerlaw_csr(M, N_COLS, alpha=alpha, hi=ZIPF_HI, seed=SEED,
-                                     nthreads=nthreads)
-    x = drb.gen.values(N_COLS, seed=SEED + 1)
+def make_workload(nthreads=0, gen=None):
+    """The power-law matrix and x.  gen: the generator module (drb.gen, or
+    oracle.gen -- the same source built into the oracle library, which the
+    reference arm uses so that it never loads the CUDA library)."""
+    if gen is None:
+        import drb
+        gen = drb.gen
+    alpha = gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
+    rp, ci, v = gen.powerlaw_csr(M, N_COLS, alpha=alpha, hi=ZIPF_HI, seed=SEED,
+                                 nthreads=nthreads)
+    x = gen.values(N_COLS, seed=SEED + 1)
     return alpha, rp, ci, v, x
 
 
@@ -195,7 +200,8 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    alpha, rp, ci, v, x = make_workload()
+    import oracle.gen
+    alpha, rp, ci, v, x = make_workload(gen=oracle.gen)
     nnz = int(rp[-1])
     bytes_ = alg_bytes(M, N_COLS, nnz, 4, 4, 4, 4, 4)
     nth, times = cpu_reference(rp, ci, v, x, args.steps, args.warmup)
@@ -318,10 +324,12 @@ def run_ours(args):
 
     # the streaming-gather floor on this pattern (column indices and values
     # streamed, x gathered at each, no rows): the roofline of a gather-bound SpMV
-    mp.gather_probe(A, xd)
-    probe_ms = statistics.mean(timed_launches(lambda: mp.gather_probe(A, xd), args.steps, stream))
-    mp.gather_probe(A, xd, False)
-    probe_cols_ms = statistics.mean(timed_launches(lambda: mp.gather_probe(A, xd, False),
+    import drb_probe
+    drb_probe.gather_probe(A, xd)
+    probe_ms = statistics.mean(timed_launches(lambda: drb_probe.gather_probe(A, xd),
+                                              args.steps, stream))
+    drb_probe.gather_probe(A, xd, False)
+    probe_cols_ms = statistics.mean(timed_launches(lambda: drb_probe.gather_probe(A, xd, False),
                                                    args.steps, stream))
 
     extra = {}

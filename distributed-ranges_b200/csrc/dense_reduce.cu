@@ -13,6 +13,8 @@
 #include <algorithm>
 #include <mutex>
 
+#include <cuda.h> // CUcontext, CUresult: types only; the library does not link libcuda
+
 #include "drb_internal.cuh"
 
 namespace drb {
@@ -412,11 +414,52 @@ constexpr int64_t kNoAllocMaxN = (int64_t)kNoAllocBlock * kNoAllocSlots; // 2^29
 static __device__ __align__(256) double g_dot_noalloc_scratch[kNoAllocSlots + 32];
 
 std::mutex g_noalloc_mu;
-void *g_noalloc_addr[64];
+struct NoAllocAddr {
+  unsigned long long ctx = 0; // id of the context the address belongs to
+  void *addr = nullptr;
+};
+NoAllocAddr g_noalloc_addr[64];
 
-// Device address of the scratch array on the current device.  Host code only
-// sees a host-side stand-in under that name, so the address is looked up once
-// per device with that device current and cached.
+// The driver's context queries, through the runtime's entry-point lookup (the
+// library does not link libcuda itself).
+typedef CUresult (*CtxCurrentFn)(CUcontext *);
+typedef CUresult (*CtxIdFn)(CUcontext, unsigned long long *);
+
+// Id of the calling thread's current context (unique for the life of the
+// process: a context created again, e.g. after cudaDeviceReset, gets a new
+// id), or 0 when none is current.  Called with g_noalloc_mu held.
+drb_status current_ctx_id(unsigned long long *id) {
+  static CtxCurrentFn cur = nullptr;
+  static CtxIdFn get_id = nullptr;
+  if (!cur || !get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    DRB_CUDA_TRY(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000,
+                                                  cudaEnableDefault, &q1));
+    DRB_CUDA_TRY(cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000,
+                                                  cudaEnableDefault, &q2));
+    if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 ||
+        !f2) {
+      set_error("drb_dot_noalloc: the driver does not provide cuCtxGetCurrent/cuCtxGetId");
+      return DRB_ERR_CUDA;
+    }
+    cur = reinterpret_cast<CtxCurrentFn>(f1);
+    get_id = reinterpret_cast<CtxIdFn>(f2);
+  }
+  CUcontext c = nullptr;
+  *id = 0;
+  if (cur(&c) != CUDA_SUCCESS || !c)
+    return DRB_OK;
+  if (get_id(c, id) != CUDA_SUCCESS)
+    *id = 0;
+  return DRB_OK;
+}
+
+// Device address of the scratch array in the current device's context.  Host
+// code only sees a host-side stand-in under that name, so the address is
+// looked up with cudaGetSymbolAddress on the first call in each context (the
+// first call on a device, and the first after its context was destroyed and
+// created again) and cached under the context's id.
 drb_status noalloc_scratch(double **out) {
   int dev = 0;
   DRB_CUDA_TRY(cudaGetDevice(&dev));
@@ -425,12 +468,17 @@ drb_status noalloc_scratch(double **out) {
     return DRB_ERR_UNSUPPORTED;
   }
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  unsigned long long id = 0;
+  DRB_TRY(current_ctx_id(&id));
+  NoAllocAddr &e = g_noalloc_addr[dev];
+  if (id == 0 || e.ctx != id || !e.addr) {
     void *p = nullptr;
-    DRB_CUDA_TRY(cudaGetSymbolAddress(&p, g_dot_noalloc_scratch));
-    g_noalloc_addr[dev] = p;
+    DRB_CUDA_TRY(cudaGetSymbolAddress(&p, g_dot_noalloc_scratch)); // makes the context
+    DRB_TRY(current_ctx_id(&id));
+    e.ctx = id;
+    e.addr = p;
   }
-  *out = static_cast<double *>(g_noalloc_addr[dev]);
+  *out = static_cast<double *>(e.addr);
   return DRB_OK;
 }
 

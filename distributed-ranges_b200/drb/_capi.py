@@ -93,7 +93,6 @@ DRB_SYMBOLS = [
     ("drb_csr_gemv", _st, [_vp, _vp, _vp, _i64, _i32, _vp]),
     ("drb_csr_gemv_host", _st, [_vp, _vp, _vp, _i64, _i32, _vp]),
     ("drb_csr_check", _st, [_vp, _vp]),
-    ("drb_csr_gather_probe", _st, [_vp, _vp, _i32, _vp]),
     ("drb_csr_variant", _st, [_vp, C.POINTER(_i32)]),
     ("drb_csr_autotune", _st, [_vp, C.POINTER(_i32), _vp]),
     ("drb_csr_residual_norm2", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),

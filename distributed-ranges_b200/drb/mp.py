@@ -736,14 +736,6 @@ def dot(a: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None,
     return out
 
 
-def gather_probe(a, x: torch.Tensor, with_values: bool = True, stream=None) -> None:
-    """drb_csr_gather_probe: stream A's column indices (and values) and gather
-    x at each -- the reads of y = A x without rows or y, a measured floor for
-    an SpMV on this pattern.  Measurement only; it computes nothing visible."""
-    check(capi.lib.drb_csr_gather_probe(a.handle, _ptr(x), int(bool(with_values)),
-                                        _stream(stream)))
-
-
 # ---- distributed_vector, iota, fill, reduce --------------------------------------
 _VEC_DT = {torch.float32: capi.DRB_F32, torch.float64: capi.DRB_F64,
            torch.int32: capi.DRB_INT32, torch.int64: capi.DRB_INT64}

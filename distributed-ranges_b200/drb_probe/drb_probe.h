@@ -1,0 +1,30 @@
+/*
+ * drb_probe.h -- the streaming-gather probe (measurement only).
+ *
+ * No counterpart in the reference, and not part of the product's C ABI
+ * (include/drb.h): lib/libdrb_probe.so exports it for the bench, which
+ * times it beside the SpMV as the floor of a gather-bound product.
+ */
+#ifndef DRB_PROBE_H
+#define DRB_PROBE_H
+
+#include "drb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Streams A's column indices (and its values when with_values != 0) with the
+ * SpMV's 16-byte loads and gathers x[col] at every nonzero: the reads of
+ * y = A x without rows, row sums or y, so its time is a floor for any SpMV on
+ * this pattern that fetches x element by element (random columns make that,
+ * not HBM, the bound).  Writes nothing the caller sees.  F32 or F64 storage
+ * (else DRB_ERR_UNSUPPORTED); x: device, n elements of the value type. */
+drb_status drb_csr_gather_probe(drb_csr_t A, const void *x, int with_values,
+                                void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRB_PROBE_H */

@@ -11,6 +11,11 @@
 // time, so its time is the roofline a gather-bound product is measured
 // against.  Nothing is written unless the running sum hits a sentinel no
 // finite input reaches (which keeps the loads live).
+//
+// Built into its own library (lib/libdrb_probe.so, linked against
+// libdrb.so for the handle's storage and error reporting), used by the bench
+// and its test only: it is not part of the C ABI of include/drb.h.
+#include "drb_probe.h"
 #include "spmv_warp.cuh"
 
 namespace drb {

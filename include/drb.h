@@ -178,16 +178,6 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
  * kernel then skipped the rest of its work; the error word is cleared). */
 drb_status drb_csr_check(drb_csr_t A, void *stream);
 
-/* Measurement only; no counterpart in the reference.  Streams A's column
- * indices (and its values when with_values != 0) with the SpMV's 16-byte
- * loads and gathers x[col] at every nonzero: the reads of y = A x without
- * rows, row sums or y, so its time is a floor for any SpMV on this pattern
- * that fetches x element by element (random columns make that, not HBM, the
- * bound).  Writes nothing the caller sees.  F32 or F64 storage; x: device,
- * n elements of the value type. */
-drb_status drb_csr_gather_probe(drb_csr_t A, const void *x, int with_values,
-                                void *stream);
-
 /* Fused residual: out[0] = || A*x - b ||_2^2 accumulated in f64 (device
  * double*), y = A*x also written when y != NULL.  k = 1. */
 drb_status drb_csr_residual_norm2(drb_csr_t A, const void *x, const void *b,
@@ -306,7 +296,10 @@ drb_status drb_dot(int64_t n, const void *a, const void *b, drb_dtype dtype,
  * it, until process exit.  Limit: n <= 2^29 (536,870,912) elements; larger n
  * returns DRB_ERR_INVALID_ARG (use drb_dot).  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress) with that
- * device current, so make that first call before any stream capture.  Every
+ * device current, so make that first call before any stream capture.  The
+ * address is kept per CUDA context: after the device's context is destroyed
+ * and created again (cudaDeviceReset), the next call looks it up again, and
+ * that call too belongs outside a capture.  Every
  * call shares the one array: calls that overlap on the GPU (different
  * streams, or different host threads) race and may return wrong sums, so
  * serialise them.  Same result contract as drb_dot (f64, deterministic for a

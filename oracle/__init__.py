@@ -17,6 +17,7 @@ REF_GEN = os.path.join(HERE, "_ref", "ref_gen")
 REF_MMREAD = os.path.join(HERE, "_ref", "ref_mmread")
 
 F32, F64 = 0, 1
+BF16 = 3  # bfloat16 bits held in uint16 arrays (the checkers only)
 I32, I64, U64 = 0, 1, 2
 ACC_T, ACC_F64, ACC_LD = 0, 1, 2
 
@@ -39,6 +40,11 @@ _SIGS = {
     "orc_csr_transpose": (_i, [_i, _i, _i64, _i64, _v, _v, _v, _v, _v, _v]),
     "orc_csr_abar": (_i, [_i, _i, _i64, _v, _v, _v, _v, _v]),
     "orc_dot": (C.c_double, [_i, _i64, _v, _v]),
+    "orc_csr_check": (_i, [_i, _i, _i, _i, _i64, _i64, _v, _v, _v, _v, _i64, _v, _i, _v, _i,
+                           _v, _v, _v, C.POINTER(C.c_double), C.POINTER(_i64)]),
+    "orc_dense_check": (_i, [_i, _i, _i, _i64, _i64, _v, _i64, _v, _i64, _v, _i,
+                             C.POINTER(C.c_double), C.POINTER(C.c_double),
+                             C.POINTER(_i64)]),
     "orc_f32_to_bf16": (None, [_i64, _v, _v]),
     "orc_bf16_to_f32": (None, [_i64, _v, _v]),
     "orc_read_matrix_market": (_i, [C.c_char_p, _i, C.POINTER(_i64), C.POINTER(_i64),
@@ -165,6 +171,68 @@ def dot(a, b):
     a = np.ascontiguousarray(a)
     b = np.ascontiguousarray(b, dtype=a.dtype)
     return float(lib.orc_dot(vcode(a.dtype), a.size, _p(a), _p(b)))
+
+
+# row-length bins of the parity statistics: [1], [2, 4], [5, 16], [17, 64],
+# [65, 256], [257, 1024], [1025, ...)
+ROW_BINS = (1, 2, 5, 17, 65, 257, 1025, 1 << 62)
+
+
+def _ecode(a) -> int:
+    return {np.dtype(np.float32): F32, np.dtype(np.float64): F64,
+            np.dtype(np.uint16): BF16}[np.dtype(a.dtype)]
+
+
+def _nthreads(n):
+    return int(n) if n else (os.cpu_count() or 1)
+
+
+def csr_check(rp, ci, v, x, m, n, y, k=1, nthreads=0, edges=ROW_BINS):
+    """Per-row error of y against the csr_row loop accumulated in long double
+    (orc_csr_check): err = |y - ref| / sum|a x| per row and right-hand side.
+    v, x: float32 / float64 / uint16 (bf16 bits) arrays; x n*k and y m*k
+    column-major.  Returns {"max", "mean", "count", "worst_row", "bins":
+    {"lo-hi": {"rows", "max", "mean"}}} (bins of row length)."""
+    assert ci.dtype == rp.dtype and ci.dtype in (np.int32, np.int64)
+    y = np.ascontiguousarray(y)
+    x = np.ascontiguousarray(x)
+    nb = len(edges) - 1
+    e = np.asarray(edges, np.int64)
+    bmax, bsum = np.zeros(nb), np.zeros(nb)
+    bcnt = np.zeros(nb, np.int64)
+    worst, wrow = C.c_double(), _i64()
+    rc = lib.orc_csr_check(_ecode(v), _ecode(x), icode(ci.dtype), _ecode(y), m, n, _p(rp),
+                           _p(ci), _p(v), _p(x), k, _p(y), _nthreads(nthreads), _p(e), nb,
+                           _p(bmax), _p(bsum), _p(bcnt), C.byref(worst), C.byref(wrow))
+    assert rc == 0, "orc_csr_check failed"
+    total = int(bcnt.sum())
+    bins = {}
+    for b in range(nb):
+        if bcnt[b]:
+            hi = "max" if e[b + 1] >= (1 << 60) else str(int(e[b + 1]) - 1)
+            bins[f"{int(e[b])}-{hi}"] = {"rows": int(bcnt[b]), "max": float(bmax[b]),
+                                         "mean": float(bsum[b] / bcnt[b])}
+    return {"max": float(worst.value), "mean": float(bsum.sum() / total) if total else 0.0,
+            "count": total, "worst_row": int(wrow.value), "bins": bins}
+
+
+def dense_check(A, x, y, k=1, n=None, nthreads=0):
+    """Per-row error of y against a long-double row-dot product: A row-major
+    (m x lda; the first n columns are the matrix), x n*k and y m*k
+    column-major; float32 / float64 / uint16 (bf16 bits) arrays.  Returns
+    {"max", "mean", "count"}."""
+    A = np.ascontiguousarray(A)
+    m, lda = A.shape
+    n = lda if n is None else n
+    x = np.ascontiguousarray(x)
+    y = np.ascontiguousarray(y)
+    mx, sm, cnt = C.c_double(), C.c_double(), _i64()
+    rc = lib.orc_dense_check(_ecode(A), _ecode(x), _ecode(y), m, n, _p(A), lda, _p(x), k,
+                             _p(y), _nthreads(nthreads), C.byref(mx), C.byref(sm),
+                             C.byref(cnt))
+    assert rc == 0, "orc_dense_check failed"
+    return {"max": float(mx.value), "mean": float(sm.value / max(cnt.value, 1)),
+            "count": int(cnt.value)}
 
 
 def f32_to_bf16_bits(a):

@@ -8,6 +8,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -709,5 +710,164 @@ int orc_read_matrix_market(const char *path, int one_indexed, int64_t *m,
 }
 
 void orc_free(void *p) { std::free(p); }
+
+} // extern "C"
+
+// ---- parity statistics ------------------------------------------------------
+namespace {
+
+inline long double elem(int t, const void *p, int64_t i) {
+  switch (t) {
+  case ORC_F32:
+    return ((const float *)p)[i];
+  case ORC_F64:
+    return ((const double *)p)[i];
+  default: {
+    uint32_t u = (uint32_t)((const uint16_t *)p)[i] << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+  }
+  }
+}
+
+inline bool type_ok(int t) { return t == ORC_F32 || t == ORC_F64 || t == ORC_BF16; }
+
+struct BinStats {
+  std::vector<double> mx, sm;
+  std::vector<int64_t> cnt;
+  double worst = -1.0;
+  int64_t worst_row = -1;
+  explicit BinStats(int nb) : mx(nb, 0.0), sm(nb, 0.0), cnt(nb, 0) {}
+  void add(int b, double e, int64_t row) {
+    if (!(e == e)) // NaN: counts as infinite
+      e = INFINITY;
+    if (b >= 0) {
+      mx[b] = std::max(mx[b], e);
+      sm[b] += e;
+      cnt[b]++;
+    }
+    if (e > worst) {
+      worst = e;
+      worst_row = row;
+    }
+  }
+  void merge(const BinStats &o) {
+    for (size_t b = 0; b < mx.size(); b++) {
+      mx[b] = std::max(mx[b], o.mx[b]);
+      sm[b] += o.sm[b];
+      cnt[b] += o.cnt[b];
+    }
+    if (o.worst > worst || (o.worst == worst && o.worst_row < worst_row)) {
+      worst = o.worst;
+      worst_row = o.worst_row;
+    }
+  }
+};
+
+inline double row_err(long double yv, long double ref, long double d) {
+  const long double diff = std::fabs(yv - ref);
+  return (double)(d > 0 ? diff / d : diff);
+}
+
+// Rows [0, m) in blocks of 4096 taken from an atomic counter by `nthreads`
+// threads; f(r0, r1, stats) accumulates into the thread's stats.
+template <class F>
+void parallel_rows(int64_t m, int nthreads, int nbins, BinStats &out, F f) {
+  const int64_t blk = 4096;
+  std::atomic<int64_t> next{0};
+  const int nt = std::max(1, nthreads);
+  std::vector<BinStats> part(nt, BinStats(std::max(nbins, 1)));
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&, t] {
+      for (;;) {
+        const int64_t r0 = next.fetch_add(blk);
+        if (r0 >= m)
+          break;
+        f(r0, std::min(m, r0 + blk), part[t]);
+      }
+    });
+  for (auto &t : th)
+    t.join();
+  for (auto &p : part)
+    out.merge(p);
+}
+
+} // namespace
+
+extern "C" {
+
+int orc_csr_check(int vtype, int xtype, int itype, int ytype, int64_t m,
+                  int64_t n, const void *rowptr, const void *colind,
+                  const void *vals, const void *x, int64_t k, const void *y,
+                  int nthreads, const int64_t *edges, int nbins, double *bmax,
+                  double *bsum, int64_t *bcount, double *worst,
+                  int64_t *worst_row) {
+  if (!type_ok(vtype) || !type_ok(xtype) || (ytype != ORC_F32 && ytype != ORC_F64) ||
+      (itype != ORC_I32 && itype != ORC_I64) || m < 0 || n < 0 || k < 1 || nbins < 0)
+    return 1;
+  auto idx = [&](const void *p, int64_t i) -> int64_t {
+    return itype == ORC_I32 ? (int64_t)((const int32_t *)p)[i] : ((const int64_t *)p)[i];
+  };
+  auto bin_of = [&](int64_t len) -> int {
+    for (int b = 0; b < nbins; b++)
+      if (len >= edges[b] && len < edges[b + 1])
+        return b;
+    return -1;
+  };
+  BinStats all(std::max(nbins, 1));
+  parallel_rows(m, nthreads, nbins, all, [&](int64_t r0, int64_t r1, BinStats &st) {
+    for (int64_t r = r0; r < r1; r++) {
+      const int64_t p0 = idx(rowptr, r), p1 = idx(rowptr, r + 1);
+      const int b = bin_of(p1 - p0);
+      for (int64_t j = 0; j < k; j++) {
+        long double s = 0, d = 0;
+        for (int64_t p = p0; p < p1; p++) {
+          const long double t = elem(vtype, vals, p) * elem(xtype, x, idx(colind, p) + j * n);
+          s += t;
+          d += std::fabs(t);
+        }
+        st.add(nbins > 0 ? b : -1, row_err(elem(ytype, y, r + j * m), s, d), r);
+      }
+    }
+  });
+  for (int b = 0; b < nbins; b++) {
+    bmax[b] = all.mx[b];
+    bsum[b] = all.sm[b];
+    bcount[b] = all.cnt[b];
+  }
+  if (worst)
+    *worst = std::max(0.0, all.worst);
+  if (worst_row)
+    *worst_row = all.worst_row;
+  return 0;
+}
+
+int orc_dense_check(int atype, int xtype, int ytype, int64_t m, int64_t n,
+                    const void *A, int64_t lda, const void *x, int64_t k,
+                    const void *y, int nthreads, double *max, double *sum,
+                    int64_t *count) {
+  if (!type_ok(atype) || !type_ok(xtype) || (ytype != ORC_F32 && ytype != ORC_F64) ||
+      m < 0 || n < 0 || k < 1 || lda < n)
+    return 1;
+  BinStats all(1);
+  parallel_rows(m, nthreads, 1, all, [&](int64_t r0, int64_t r1, BinStats &st) {
+    for (int64_t r = r0; r < r1; r++)
+      for (int64_t j = 0; j < k; j++) {
+        long double s = 0, d = 0;
+        for (int64_t c = 0; c < n; c++) {
+          const long double t = elem(atype, A, r * lda + c) * elem(xtype, x, c + j * n);
+          s += t;
+          d += std::fabs(t);
+        }
+        st.add(0, row_err(elem(ytype, y, r + j * m), s, d), r);
+      }
+  });
+  *max = all.mx[0];
+  *sum = all.sm[0];
+  *count = all.cnt[0];
+  return 0;
+}
 
 } // extern "C"

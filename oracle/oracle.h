@@ -116,6 +116,41 @@ int orc_csr_abar(int vtype, int itype, int64_t m, const void *rowptr,
 /* sum_i a[i]*b[i] accumulated in long double, returned as double. */
 double orc_dot(int vtype, int64_t n, const void *a, const void *b);
 
+/* ---- parity statistics (the checker at full sizes) ----------------------- */
+
+/* Element-type codes of the checkers: ORC_F32, ORC_F64, or ORC_BF16 (bfloat16
+ * bits, widened exactly to float). */
+enum { ORC_BF16 = 3 };
+
+/* Per-row error of a result y against the csr_row loop
+ * (csr_row_distribution.hpp:116-133), for every row r and right-hand side j:
+ *   ref = sum_p a_p * x[col_p + j*n]     accumulated in long double,
+ *   d   = sum_p |a_p * x[col_p + j*n]|   (long double),
+ *   err = |y[r + j*m] - ref| / d          (|y - ref| when d == 0).
+ * vtype / xtype: element types of the values and of x (F32 | F64 | BF16);
+ * itype: of rowptr and colind (I32 | I64); ytype: of y (F32 | F64).  x is
+ * n*k column-major, y m*k column-major (k = 1: plain vectors).  Rows are split
+ * over `nthreads` threads.  Statistics per bin of row length (rows of length
+ * L with edges[b] <= L < edges[b+1], b < nbins): bmax[b], bsum[b] (sum of
+ * err, for the mean), bcount[b] (row x rhs pairs); *worst = the largest err
+ * over all rows and *worst_row its row.  NaN in y counts as an infinite err.
+ * Returns 0, or 1 on an unsupported type code. */
+int orc_csr_check(int vtype, int xtype, int itype, int ytype, int64_t m,
+                  int64_t n, const void *rowptr, const void *colind,
+                  const void *vals, const void *x, int64_t k, const void *y,
+                  int nthreads, const int64_t *edges, int nbins, double *bmax,
+                  double *bsum, int64_t *bcount, double *worst,
+                  int64_t *worst_row);
+
+/* The same statistics for a dense row-major A (m x n, leading dimension lda,
+ * element type atype = F32 | F64 | BF16), x n*k and y m*k column-major:
+ * ref_r = sum_c A[r*lda + c] * x[c + j*n] in long double, d = sum |.|.
+ * One bin (all rows): *max, *sum, *count. */
+int orc_dense_check(int atype, int xtype, int ytype, int64_t m, int64_t n,
+                    const void *A, int64_t lda, const void *x, int64_t k,
+                    const void *y, int nthreads, double *max, double *sum,
+                    int64_t *count);
+
 /* ---- bf16 helpers -------------------------------------------------------- */
 
 /* Round-to-nearest-even float -> bfloat16 bits (NaN kept quiet). */

@@ -183,4 +183,3 @@ def test_vector_and_cg_entry_points_reject_bad_arguments_without_gpu():
     info = capi.CgInfo()
     assert lib.drb_csr_cg(None, None, None, 10, 1e-6, C.byref(info), None) == \
         capi.DRB_ERR_INVALID_ARG
-    assert lib.drb_csr_gather_probe(None, None, 1, None) == capi.DRB_ERR_INVALID_ARG

@@ -500,8 +500,9 @@ def test_gather_probe_runs_and_checks_storage(mp, dtype, index):
     y0 = torch.empty(m, dtype=x.dtype, device="cuda")
     a.gemv_device(x, y0)
     x0 = x.clone()
-    mp.gather_probe(a, x)
-    mp.gather_probe(a, x, with_values=False)
+    import drb_probe
+    drb_probe.gather_probe(a, x)
+    drb_probe.gather_probe(a, x, with_values=False)
     y1 = torch.empty_like(y0)
     a.gemv_device(x, y1)
     assert torch.equal(x, x0) and torch.equal(y0, y1)
@@ -509,7 +510,7 @@ def test_gather_probe_runs_and_checks_storage(mp, dtype, index):
     vb = v.astype(np.float32)
     b16 = mp.distributed_sparse_matrix(mp.csr_matrix_view(vb, rp, ci, (m, n)), 0,
                                        storage=torch.bfloat16)
-    rc = capi.lib.drb_csr_gather_probe(b16.handle, C.c_void_p(x.data_ptr()), 1, None)
+    rc = drb_probe.lib.drb_csr_gather_probe(b16.handle, C.c_void_p(x.data_ptr()), 1, None)
     assert rc == capi.DRB_ERR_UNSUPPORTED
 
 

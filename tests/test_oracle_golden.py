@@ -164,3 +164,26 @@ def test_all_fixtures_have_sources():
     assert len(files) >= 10
     for p in files:
         assert "source" in np.load(p).files
+
+
+@pytest.mark.parametrize("kind", ["powerlaw", "uniform_rows", "values"])
+def test_oracle_generator_copy_matches_product_generator(kind):
+    """The bench's reference arm builds its inputs with oracle.gen (the
+    package's generate.cpp linked into the oracle library): the same bytes
+    as drb.gen for the same seeds, whatever the thread count."""
+    import drb
+    import oracle.gen as og
+    if kind == "powerlaw":
+        a = og.zipf_alpha_for_mean(1, 512, 20.0)
+        assert a == drb.gen.zipf_alpha_for_mean(1, 512, 20.0)
+        got = og.powerlaw_csr(3000, 5000, alpha=a, hi=512, seed=11, nthreads=3)
+        ref = drb.gen.powerlaw_csr(3000, 5000, alpha=a, hi=512, seed=11, nthreads=1)
+    elif kind == "uniform_rows":
+        got = og.uniform_rows_csr(2000, 2000, lo=8, hi=64, seed=12, value_dtype=np.float64)
+        ref = drb.gen.uniform_rows_csr(2000, 2000, lo=8, hi=64, seed=12,
+                                       value_dtype=np.float64)
+    else:
+        got = (og.values(100_003, seed=13, dist=og.NORMAL_ROWSCALE),)
+        ref = (drb.gen.values(100_003, seed=13, dist=drb.gen.NORMAL_ROWSCALE),)
+    for g, r in zip(got, ref):
+        assert g.dtype == r.dtype and g.tobytes() == r.tobytes()
