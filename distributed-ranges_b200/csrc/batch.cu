@@ -199,13 +199,33 @@ __device__ __forceinline__ int clog2(int x) {
 
 constexpr int kUnroll = 4; // X gathers in flight per lane
 
+// BF16 storage sums two-sum compensated, per block of the kUnroll products a
+// lane has in flight: the block is one chain of fused multiply-adds (at most
+// kUnroll roundings, each within u of the block's sum of |a x|), and the
+// block sum enters the row's running sum through a two-sum whose exact error
+// goes to a compensation term, added when the row completes.  So a row's
+// error stays within about (kUnroll + 1) u of sum |a x| however long the row
+// (plain f32 sums grow with its length), for about a third of the
+// arithmetic of a two-sum per product.  The operations are the _rn
+// intrinsics, which the compiler never contracts or reorders.
+template <class V> struct Comp {
+  static constexpr bool value = sizeof(V) == 2;
+};
+
+__device__ __forceinline__ void two_sum_rn(float a, float b, float &s, float &e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
 // The nonzeros [b, e) of one row staged at shared addresses colS/valS (byte
-// address of stage element 0), this lane's VEC sums; the lane takes b, b +
-// step, ... with kUnroll gathers in flight.
+// address of stage element 0), this lane's VEC sums (and, compensated, their
+// error terms cmp); the lane takes b, b + step, ... with kUnroll gathers in
+// flight.
 template <class V, class XT, int VEC, class A>
 __device__ __forceinline__ void row_sums(uint32_t colS, uint32_t valS, int b,
                                          int e, const XT *Xl, int ldx,
-                                         int step, A (&acc)[VEC]) {
+                                         int step, A (&acc)[VEC], A (&cmp)[VEC]) {
   for (int q = b; q < e; q += kUnroll * step) {
     XWords<XT, VEC> xv[kUnroll];
     A vv[kUnroll];
@@ -217,12 +237,39 @@ __device__ __forceinline__ void row_sums(uint32_t colS, uint32_t valS, int b,
       vv[u] = q + u * step < e ? v : A(0);
       ldg_x<XT, VEC>(Xl + (int64_t)col * ldx, xv[u]);
     }
+    if constexpr (Comp<V>::value) {
 #pragma unroll
-    for (int u = 0; u < kUnroll; u++) {
+      for (int t = 0; t < VEC; t++) {
+        float blk = __fmul_rn(vv[0], x_at<XT, VEC, A>(xv[0], t));
+#pragma unroll
+        for (int u = 1; u < kUnroll; u++)
+          blk = __fmaf_rn(vv[u], x_at<XT, VEC, A>(xv[u], t), blk);
+        float s, err;
+        two_sum_rn(acc[t], blk, s, err);
+        acc[t] = s;
+        cmp[t] = __fadd_rn(cmp[t], err);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < kUnroll; u++) {
 #pragma unroll
         for (int t = 0; t < VEC; t++)
           acc[t] = fma(vv[u], (x_at<XT, VEC, A>(xv[u], t)), acc[t]);
+      }
     }
+  }
+}
+
+// acc += other lane's (acc2, cmp2): compensated when the storage is BF16.
+template <class V, class A>
+__device__ __forceinline__ void merge_sum(A &acc, A &cmp, A acc2, A cmp2) {
+  if constexpr (Comp<V>::value) {
+    float s, err;
+    two_sum_rn(acc, acc2, s, err);
+    acc = s;
+    cmp = __fadd_rn(cmp, __fadd_rn(cmp2, err));
+  } else {
+    acc += acc2;
   }
 }
 
@@ -312,23 +359,26 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
       const uint32_t rsP = wsm + a.rs_off + st * a.rs_stage + 4 * (r0 & 3);
       for (int i0 = 0; i0 < nrows; i0 += R) {
         const int i = i0 + grp;
-        A acc[VEC];
+        A acc[VEC], cmp[VEC];
 #pragma unroll
         for (int t = 0; t < VEC; t++)
-          acc[t] = 0;
+          acc[t] = cmp[t] = 0;
         if (con && row_on && i < nrows) {
           const int b = lds_s32(rsP + 4 * i) - p0, e = lds_s32(rsP + 4 * i + 4) - p0;
-          row_sums<V, XT, VEC, A>(colP, valP, b + gs, e, Xl, ldx, G, acc);
+          row_sums<V, XT, VEC, A>(colP, valP, b + gs, e, Xl, ldx, G, acc, cmp);
         }
         for (int dd = 1; dd < G; dd <<= 1) {
 #pragma unroll
-          for (int t = 0; t < VEC; t++)
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], dd * KP);
+          for (int t = 0; t < VEC; t++) {
+            const A a2 = __shfl_xor_sync(0xffffffffu, acc[t], dd * KP);
+            const A c2 = Comp<V>::value ? __shfl_xor_sync(0xffffffffu, cmp[t], dd * KP) : A(0);
+            merge_sum<V>(acc[t], cmp[t], a2, c2);
+          }
         }
         if (con && row_on && gs == 0 && i < nrows) {
 #pragma unroll
           for (int t = 0; t < VEC; t++)
-            ytile[i * ystride + jj * VEC + t] = acc[t];
+            ytile[i * ystride + jj * VEC + t] = Comp<V>::value ? acc[t] + cmp[t] : acc[t];
         }
       }
       __syncwarp();
@@ -357,10 +407,10 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
     } else {
       // ---- one long row, staged cap nonzeros at a time into stage st ----
       const int64_t lo0 = bm->rowptr[r0], hi0 = bm->rowptr[r0 + 1];
-      A acc[VEC];
+      A acc[VEC], cmp[VEC];
 #pragma unroll
       for (int t = 0; t < VEC; t++)
-        acc[t] = 0;
+        acc[t] = cmp[t] = 0;
       for (int64_t lo = lo0; lo < hi0; lo += a.cap) {
         const int len = (int)min((int64_t)a.cap, hi0 - lo);
         copy16s<int32_t>(colS, bm->colind, lo, len, lane);
@@ -371,26 +421,28 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
         if (con)
           row_sums<V, XT, VEC, A>(colS + 4 * (int)(lo & 3),
                                   valS + (uint32_t)sizeof(V) * (int)(lo & VOFF_MASK),
-                                  slot, len, Xl, ldx, S, acc);
+                                  slot, len, Xl, ldx, S, acc, cmp);
         __syncwarp();
       }
       for (int dd = 1; dd < S; dd <<= 1) {
 #pragma unroll
         for (int t = 0; t < VEC; t++) {
           const A o = __shfl_down_sync(0xffffffffu, acc[t], dd * KP);
+          const A oc = Comp<V>::value ? __shfl_down_sync(0xffffffffu, cmp[t], dd * KP) : A(0);
           if ((slot & (2 * dd - 1)) == 0 && slot + dd < S)
-            acc[t] += o;
+            merge_sum<V>(acc[t], cmp[t], o, oc);
         }
       }
       if (slot == 0 && con) {
 #pragma unroll
         for (int t = 0; t < VEC; t++) {
           const int c = c0 + t;
+          const A yv = Comp<V>::value ? acc[t] + cmp[t] : acc[t];
           if (c < k) {
             if (a.row_major)
-              Y[(int64_t)r0 * k + c] = acc[t];
+              Y[(int64_t)r0 * k + c] = yv;
             else
-              Y[(int64_t)r0 + (int64_t)c * m] = acc[t];
+              Y[(int64_t)r0 + (int64_t)c * m] = yv;
           }
         }
       }

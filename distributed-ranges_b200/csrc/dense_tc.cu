@@ -23,10 +23,12 @@
 // below the tensor-core roofline), so the design goal is a full TMA ring per
 // SM.  No load uses cluster multicast.
 //
-// Every mbarrier wait gives up after one second of %globaltimer: the CTA
-// then records DRB_ERR_TIMEOUT in the launch's error word and leaves its
-// loops; the producer and MMA loops of every CTA test the word before each
-// stage, so later CTAs skip their work, and tensor memory is always freed.
+// Every mbarrier wait gives up after one second of %globaltimer (a plan can
+// shorten the limit): the CTA then records DRB_ERR_TIMEOUT in the launch's
+// error word and leaves its loops; the producer and MMA lanes test the word
+// before each stage and while they wait, so the other CTAs stop early.
+// Before a CTA exits, its producer waits (bounded) until every bulk copy it
+// issued has landed, and tensor memory is always freed.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -68,6 +70,8 @@ struct DArgs {
   int tmem_cols;     // power of two >= max(32, N)
   int row_major;
   int *err;
+  uint64_t wait_ns; // limit of every mbarrier wait
+  int stall_tile;   // failure-detection hook: this CTA issues no loads (-1: none)
 };
 
 // ---- tcgen05 / TMA PTX wrappers --------------------------------------------
@@ -149,6 +153,21 @@ __device__ __forceinline__ bool aborted(const int *err, volatile int *flag) {
   return *flag != 0 || *(volatile const int *)err != 0;
 }
 
+// Pipeline wait of the producer and MMA lanes: true when the phase
+// completed.  False when the CTA must stop: this CTA's flag or the launch's
+// error word was set meanwhile (by the other lane or another CTA), or the
+// limit ran out (then recorded here as DRB_ERR_TIMEOUT).
+__device__ __forceinline__ bool pipe_wait(uint64_t *bar, uint32_t parity, const DArgs &a,
+                                          volatile int *flag) {
+  const int r = tma::mbar_wait_or_stop(bar, parity, a.wait_ns, flag,
+                                       (const volatile int *)a.err);
+  if (r == 2) {
+    *flag = 1;
+    atomicExch(a.err, DRB_ERR_TIMEOUT);
+  }
+  return r == 0;
+}
+
 template <int kStages, int kBoxes>
 __global__ void __launch_bounds__(kThreads, 1) dense_tc(const DArgs a) {
   extern __shared__ unsigned char raw_smem[];
@@ -199,26 +218,36 @@ __global__ void __launch_bounds__(kThreads, 1) dense_tc(const DArgs a) {
   if (warp == 0) {
     if (lane == 0) {
       const uint32_t tx = (uint32_t)(kStageA + stage_b);
-      for (int s = 0; s < nk; s++) {
-        const int slot = s % kStages;
-        const uint32_t ph = (uint32_t)((s / kStages) & 1);
-        if (aborted(a.err, abort_flag))
-          break;
-        if (!tma::mbar_wait(&empty[slot], ph ^ 1)) {
-          *abort_flag = 1;
-          atomicExch(a.err, DRB_ERR_TIMEOUT);
-          break;
-        }
-        tma::mbar_arrive_expect_tx(&full[slot], tx);
+      int issued = 0; // stages whose loads were issued
+      if ((int)blockIdx.x != a.stall_tile) {
+        for (int s = 0; s < nk; s++) {
+          const int slot = s % kStages;
+          const uint32_t ph = (uint32_t)((s / kStages) & 1);
+          if (aborted(a.err, abort_flag))
+            break;
+          if (!pipe_wait(&empty[slot], ph ^ 1, a, abort_flag))
+            break;
+          tma::mbar_arrive_expect_tx(&full[slot], tx);
 #pragma unroll
-        for (int b = 0; b < kBoxes; b++) {
-          const int kx = (s * kBoxes + b) * kTileK;
-          tma_load_2d(sa + slot * kStageA + b * kABytes, mt.tma, kx, tile.y,
-                      &full[slot]);
-          tma_load_2d(sb + slot * stage_b + b * bbytes, mt.tmx, kx, 0,
-                      &full[slot]);
+          for (int b = 0; b < kBoxes; b++) {
+            const int kx = (s * kBoxes + b) * kTileK;
+            tma_load_2d(sa + slot * kStageA + b * kABytes, mt.tma, kx, tile.y,
+                        &full[slot]);
+            tma_load_2d(sb + slot * stage_b + b * bbytes, mt.tmx, kx, 0,
+                        &full[slot]);
+          }
+          issued = s + 1;
         }
       }
+      // No bulk copy may still be writing this CTA's shared memory when it
+      // exits: wait (bounded) for the last phase armed on every slot.  After
+      // a normal run the MMA lane has consumed them all and these return at
+      // once; after an abort they cover the stages it never reached.
+      for (int s = issued > kStages ? issued - kStages : 0; s < issued; s++)
+        if (!tma::mbar_wait(&full[s % kStages], (uint32_t)((s / kStages) & 1))) {
+          *abort_flag = 1;
+          atomicExch(a.err, DRB_ERR_TIMEOUT);
+        }
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -228,11 +257,8 @@ __global__ void __launch_bounds__(kThreads, 1) dense_tc(const DArgs a) {
         const uint32_t ph = (uint32_t)((s / kStages) & 1);
         if (aborted(a.err, abort_flag))
           break;
-        if (!tma::mbar_wait(&full[slot], ph)) {
-          *abort_flag = 1;
-          atomicExch(a.err, DRB_ERR_TIMEOUT);
+        if (!pipe_wait(&full[slot], ph, a, abort_flag))
           break;
-        }
         tc_fence_after();
 #pragma unroll
         for (int b = 0; b < kBoxes; b++) {
@@ -252,6 +278,8 @@ __global__ void __launch_bounds__(kThreads, 1) dense_tc(const DArgs a) {
   } else {
     // epilogue: warp w owns TMEM lanes 32*(w%4) .. +31 = tile rows
     const int q = warp & 3;
+    // the MMA lane always commits `done` (also after an abort), so this wait
+    // keeps the fixed one-second limit whatever the plan's pipeline limit
     const bool ok = tma::mbar_wait(done, 0);
     if (!ok) {
       *abort_flag = 1;
@@ -281,6 +309,11 @@ __global__ void __launch_bounds__(kThreads, 1) dense_tc(const DArgs a) {
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
+    // every MMA has completed before the accumulator is freed (immediate
+    // unless the epilogue gave up on `done`)
+    if (lane == 0 && !tma::mbar_wait(done, 0))
+      atomicExch(a.err, DRB_ERR_TIMEOUT);
+    __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
                      tmem),
@@ -383,6 +416,8 @@ struct DenseBatch {
   int npacks = 0;
   int64_t max_n = 0;
   std::vector<std::pair<float *, size_t>> zero; // outputs of n == 0 matrices
+  uint64_t wait_ns = tma::kWaitNs;
+  int stall_tile = -1;
   DevBuf maps, mats, tiles, xp, packs, err;
 };
 
@@ -527,6 +562,8 @@ drb_status dense_batch_launch(DenseBatch &P, cudaStream_t s) {
   a.tmem_cols = P.tmem_cols;
   a.row_major = P.row_major ? 1 : 0;
   a.err = P.err.as<int>();
+  a.wait_ns = P.wait_ns;
+  a.stall_tile = P.stall_tile;
   dense_kernel(P.variant)<<<P.ntiles, kThreads, P.smem, s>>>(a);
   DRB_CUDA_TRY(cudaGetLastError());
   note_launch(2);
@@ -580,6 +617,18 @@ drb_status drb_dense_batch_set_variant(drb_dense_batch_t P, int variant) {
     return fail(DRB_ERR_INVALID_ARG, "invalid argument: plan is NULL");
   DeviceGuard g(P->device);
   return set_dense_variant(*P, variant);
+}
+
+drb_status drb_dense_batch_set_wait(drb_dense_batch_t P, uint64_t wait_ns,
+                                    int32_t stall_tile) {
+  clear_error();
+  if (!P)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: plan is NULL");
+  if (stall_tile < -1)
+    return fail(DRB_ERR_INVALID_ARG, "invalid argument: stall_tile %d", (int)stall_tile);
+  P->wait_ns = wait_ns ? wait_ns : tma::kWaitNs;
+  P->stall_tile = stall_tile;
+  return DRB_OK;
 }
 
 drb_status drb_dense_batch_check(drb_dense_batch_t P, void *stream) {

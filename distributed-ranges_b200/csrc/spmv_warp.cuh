@@ -94,11 +94,19 @@ template <class T> __device__ __forceinline__ T wsum(T v) {
   return v;
 }
 
+// Additions that the compiler may not contract with a preceding multiply
+// into a fused multiply-add (an error-free transformation needs each
+// operation rounded on its own).
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
 // Knuth's two-sum: s + e == a + b exactly, s = fl(a + b).
 template <class T> __device__ __forceinline__ void two_sum(T a, T b, T &s, T &e) {
-  s = a + b;
-  const T bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
+  s = add_rn(a, b);
+  const T bb = sub_rn(s, a);
+  e = add_rn(sub_rn(a, sub_rn(s, bb)), sub_rn(b, bb));
 }
 
 // Compensated accumulator (running sum and error term).

@@ -1,6 +1,7 @@
 // spmv_warp_bf16.cu -- instantiates the persistent SpMV for bfloat16 values:
-// x in bf16 (or in fp32 with DRB_FLAG_BF16_X_F32), products exact in fp32,
-// two-sum compensated fp32 sums, y in fp32.
+// x in bf16 (or in fp32 with DRB_FLAG_BF16_X_F32), two-sum compensated fp32
+// sums, y in fp32.  A bf16 x bf16 product is exact in fp32; a bf16 x fp32
+// product rounds once (relative 2^-24) before the compensated sum.
 #include "spmv_warp.cuh"
 
 namespace drb {

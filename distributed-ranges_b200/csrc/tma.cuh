@@ -57,8 +57,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Wait for the phase with the given parity to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+// Wait for the phase with the given parity to complete; false once
+// `limit_ns` nanoseconds have passed without it.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          uint64_t limit_ns = kWaitNs) {
   if (mbar_try_wait(bar, parity))
     return true;
   const uint64_t t0 = globaltimer();
@@ -66,8 +68,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     for (int i = 0; i < 64; i++)
       if (mbar_try_wait(bar, parity))
         return true;
-    if (globaltimer() - t0 > kWaitNs)
+    if (globaltimer() - t0 > limit_ns)
       return false;
+  }
+}
+
+// As mbar_wait, but also gives up (returning 1) as soon as *stop or *stop2
+// becomes non-zero; 0 = the phase completed, 2 = the limit ran out.
+__device__ __forceinline__ int mbar_wait_or_stop(uint64_t *bar, uint32_t parity,
+                                                 uint64_t limit_ns,
+                                                 const volatile int *stop,
+                                                 const volatile int *stop2) {
+  if (mbar_try_wait(bar, parity))
+    return 0;
+  const uint64_t t0 = globaltimer();
+  for (;;) {
+    for (int i = 0; i < 64; i++)
+      if (mbar_try_wait(bar, parity))
+        return 0;
+    if (*stop || *stop2)
+      return 1;
+    if (globaltimer() - t0 > limit_ns)
+      return 2;
   }
 }
 

@@ -115,6 +115,7 @@ DRB_SYMBOLS = [
     ("drb_dense_batch_gemv", _st, [_vp, _vp]),
     ("drb_dense_batch_set_variant", _st, [_vp, _i32]),
     ("drb_dense_batch_check", _st, [_vp, _vp]),
+    ("drb_dense_batch_set_wait", _st, [_vp, C.c_uint64, _i32]),
     ("drb_dense_batch_destroy", _st, [_vp]),
     ("drb_dot", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),
     ("drb_dot_noalloc", _st, [_i64, _vp, _vp, _i32, _vp, _vp]),

@@ -9,10 +9,15 @@ rows they touch (found by upper_bound over rowptr, :253-272), so a row may be
 split between ranks.  x is replicated on every rank (broadcasted_vector);
 each rank multiplies its segment on its own GPU with the single-process
 kernels, and the partial results are gathered and assembled as the
-reference's gather_gemv_vector does: csr_row copies each rank's rows into
-place (:159-204); csr_eq zero-fills the result, adds each rank's first row
-(the one a previous rank may also hold) and copies the rest, in rank order
-(csr_eq_distribution.hpp:159-216).
+reference's gather_gemv_vector does: with a root, only the root receives
+the ranks' blocks (the reference's MPI_Gather_c / MPI_Gatherv_c,
+csr_row_distribution.hpp:159-168, csr_eq_distribution.hpp:175); without one
+(the reference's gemv + broadcast) every rank does.  csr_row copies each
+rank's rows into place (:159-204); csr_eq zero-fills the result, adds each
+rank's first row (the one a previous rank may also hold) and copies the
+rest, in rank order (csr_eq_distribution.hpp:159-216).  The assembly runs on
+the receiving rank's device (the GPU under NCCL), vectorised over the
+right-hand sides.
 
 Set-up follows the reference's init: the root broadcasts the shape and the
 per-rank segment table (the reference's val_information broadcast) and
@@ -104,7 +109,7 @@ class ShardedCsr:
         if not 0 <= self.root < P:
             raise ValueError(f"root {root} is not a rank of {P}")
         dev = comm.device()
-        meta = torch.zeros(4, dtype=torch.int64, device=dev)
+        meta = torch.zeros(5, dtype=torch.int64, device=dev)
         if rank == self.root:
             vals = np.ascontiguousarray(view.values_data())
             rp = np.ascontiguousarray(view.rowptr_data()).astype(np.int64)
@@ -112,11 +117,14 @@ class ShardedCsr:
             m, n = view.shape()
             if vals.dtype not in _VCODE:
                 raise TypeError(f"values dtype {vals.dtype} (need float32/float64)")
-            meta[:] = torch.tensor([m, n, int(rp[m]) if m else 0, _VCODE[vals.dtype]])
+            # column indices travel as int32 whenever the columns fit
+            wide = int(n >= 2**31 - 1)
+            meta[:] = torch.tensor([m, n, int(rp[m]) if m else 0, _VCODE[vals.dtype], wide])
         comm.bcast(meta, self.root)
-        m, n, nnz, vcode = (int(v) for v in meta.cpu())
+        m, n, nnz, vcode, wide = (int(v) for v in meta.cpu())
         self.m, self.n, self.nnz = m, n, nnz
         self.np_dtype, self.dtype = _VDT[vcode]
+        ci_np, ci_t = (np.int64, torch.int64) if wide else (np.int32, torch.int32)
         table = torch.zeros((P, 4), dtype=torch.int64, device=dev)
         if rank == self.root:
             table[:] = torch.from_numpy(segment_table(rp, m, nnz, P, self.eq))
@@ -130,7 +138,8 @@ class ShardedCsr:
             for r in range(P):
                 a0, a1, b0, b1 = (int(v) for v in self.table[r])
                 lrp = np.clip(rp[a0:a1 + 1], b0, b1) - b0 if a1 > a0 else np.zeros(1, np.int64)
-                parts = (lrp.astype(np.int64), ci[b0:b1].astype(np.int64), vals[b0:b1])
+                parts = (lrp.astype(np.int64), ci[b0:b1].astype(ci_np, copy=False),
+                         vals[b0:b1])
                 if r == rank:
                     lrp_l, lci, lv = parts
                     continue
@@ -140,7 +149,7 @@ class ShardedCsr:
                                   dst=comm.global_rank(r), group=comm.group)
         else:
             lrp_t = torch.empty(max(rows, 0) + 1, dtype=torch.int64, device=dev)
-            lci_t = torch.empty(cnt, dtype=torch.int64, device=dev)
+            lci_t = torch.empty(cnt, dtype=ci_t, device=dev)
             lv_t = torch.empty(cnt, dtype=self.dtype, device=dev)
             for t in (lrp_t, lci_t, lv_t):
                 if t.numel():
@@ -162,8 +171,11 @@ class ShardedCsr:
     # ---- gemv: local product + gather (gather_gemv_vector) -----------------------
     def gemv(self, root, res, x: torch.Tensor, k: int) -> None:
         """y = A x for k column-major right-hand sides; the result is
-        assembled into `res` (m*k, column-major) on `root`, or on every rank
-        when root is None (the reference's no-root gemv)."""
+        assembled into `res` (m*k, column-major) on `root` only, or on every
+        rank when root is None (the reference's no-root gemv).  Every rank's
+        block is padded to the largest segment (the reference gathers
+        ceil(m/P) rows per rank too).  last_gather_bytes: the bytes this
+        rank received in the gather."""
         comm, P = self.comm, self.comm.size()
         rank = comm.rank()
         dev = comm.device()
@@ -172,28 +184,40 @@ class ShardedCsr:
         if self.local is not None:
             y = self.local.gemv(x, k)
             buf[: self.rows * k] = y.reshape(-1).to(dtype=self.dtype, device=dev)
-        parts = [torch.empty_like(buf) for _ in range(P)]
-        dist.all_gather(parts, buf, group=comm.group)
-        if root is not None and rank != int(root):
-            return
+        block_bytes = buf.numel() * buf.element_size()
+        if root is None:
+            parts = [torch.empty_like(buf) for _ in range(P)]
+            dist.all_gather(parts, buf, group=comm.group)
+            self.last_gather_bytes = (P - 1) * block_bytes
+        else:
+            root = int(root)
+            on_root = rank == root
+            parts = [torch.empty_like(buf) for _ in range(P)] if on_root else None
+            dist.gather(buf, gather_list=parts, dst=comm.global_rank(root), group=comm.group)
+            self.last_gather_bytes = (P - 1) * block_bytes if on_root else 0
+            if not on_root:
+                return
+        _write(res, self._assemble(parts, k))
+
+    def _assemble(self, parts, k: int) -> torch.Tensor:
+        """The gathered blocks (rank r: its rows x k, column-major) placed
+        into y (m x k, column-major) on their device, in rank order."""
         m = self.m
-        out = np.zeros(m * k, self.np_dtype)
-        host = [p.cpu().numpy() for p in parts]
-        for r in range(P):
+        out = torch.zeros((k, m), dtype=self.dtype, device=parts[0].device)
+        for r in range(len(parts)):
             r0, r1 = int(self.table[r, 0]), int(self.table[r, 1])
             nr = r1 - r0
             if nr <= 0:
                 continue
-            g = host[r]
-            for j in range(k):
-                col = g[j * nr:(j + 1) * nr]
-                if self.eq:
-                    # add the first row (it may be split), copy the rest
-                    out[r0 + j * m] = out[r0 + j * m] + col[0]
-                    out[r0 + 1 + j * m:r1 + j * m] = col[1:]
-                else:
-                    out[r0 + j * m:r1 + j * m] = col
-        _write(res, out)
+            blk = parts[r][: nr * k].view(k, nr)
+            if self.eq:
+                # add the first row (a previous rank may hold part of it),
+                # copy the rest
+                out[:, r0] += blk[:, 0]
+                out[:, r0 + 1:r1] = blk[:, 1:]
+            else:
+                out[:, r0:r1] = blk
+        return out.view(-1)
 
     # ---- entries of every rank (iteration) -----------------------------------------
     def all_entries(self):
@@ -223,13 +247,17 @@ class ShardedCsr:
         return np.concatenate(R), np.concatenate(Cc), np.concatenate(V)
 
 
-def _write(res, out: np.ndarray) -> None:
+def _write(res, out: torch.Tensor) -> None:
+    """y (a flat tensor) into the caller's result: a numpy array or list on
+    the host, or a tensor on any device."""
+    if isinstance(res, torch.Tensor):
+        res.copy_(out.view(res.shape))
+        return
+    host = out.cpu().numpy()
     if isinstance(res, np.ndarray):
-        res[...] = out.reshape(res.shape)
-    elif isinstance(res, torch.Tensor):
-        res.copy_(torch.from_numpy(out).view(res.shape))
+        res[...] = host.reshape(res.shape)
     else:
-        res[:] = out.tolist()
+        res[:] = host.tolist()
 
 
 def broadcast_tensor(comm: DistComm, root: int, data, size: int, dtype=None) -> torch.Tensor:

@@ -714,6 +714,12 @@ class dense_batch:
     def check(self, stream=None) -> None:
         check(capi.lib.drb_dense_batch_check(self._p, _stream(stream)))
 
+    def set_wait(self, wait_ns: int = 0, stall_tile: int = -1) -> None:
+        """drb_dense_batch_set_wait: limit the in-kernel waits of later
+        launches to wait_ns (0 = one second); stall_tile >= 0 makes that
+        tile's CTA issue no loads (failure detection)."""
+        check(capi.lib.drb_dense_batch_set_wait(self._p, int(wait_ns), int(stall_tile)))
+
     def destroy(self) -> None:
         if self._p and self._p.value:
             capi.lib.drb_dense_batch_destroy(self._p)

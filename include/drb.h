@@ -142,8 +142,9 @@ drb_status drb_csr_get_entries(drb_csr_t A, int64_t offset, int64_t count,
 
 /* y = A * x for k right-hand sides, device pointers.  Element types: x and y
  * have the storage type, except BF16 storage: x bf16 (f32 with
- * DRB_FLAG_BF16_X_F32), y f32, products exact in f32 (k = 1: summed with
- * two-sum compensation; k > 1: plain f32 sums, as drb_batch_*).  k > 1 runs
+ * DRB_FLAG_BF16_X_F32), y f32, row sums two-sum compensated in f32 (k = 1:
+ * per product, a bf16 x bf16 product being exact in f32 and a bf16 x f32 one
+ * rounding once; k > 1: per block of four products, as drb_batch_*).  k > 1 runs
  * the batched SpMM kernel on a batch of this one handle, built on the first
  * call with a given (k, layout) -- that call synchronises `stream`, and the
  * handle then keeps a row-major copy of X (n * k elements, rows padded to 16
@@ -205,7 +206,9 @@ drb_status drb_csr_update_values(drb_csr_t A, const void *values,
  * matrices at once.  X_i is n_i x k and Y_i is m_i x k, both in `layout`
  * (DRB_COL_MAJOR is the reference's slim-matrix layout, x[c + j*n]).
  * Element types as drb_csr_gemv: the storage type, or for BF16 storage bf16
- * X (f32 with DRB_FLAG_BF16_X_F32) and f32 Y; BF16 sums are plain f32.
+ * X (f32 with DRB_FLAG_BF16_X_F32) and f32 Y; BF16 sums are two-sum
+ * compensated f32, per block of four products (a fused multiply-add chain per
+ * block): a row's error stays within about 5 f32 roundings of sum |a x|.
  * Handles must share the device and the storage type, have 32-bit rowptr and
  * column indices (nnz < 2^31 each), and must outlive the batch. */
 typedef struct drb_batch_plan *drb_batch_t;
@@ -279,6 +282,15 @@ drb_status drb_dense_batch_set_variant(drb_dense_batch_t P, int variant);
 /* Synchronise `stream`; DRB_ERR_TIMEOUT when a bounded in-kernel wait of an
  * earlier launch expired (the error word is cleared). */
 drb_status drb_dense_batch_check(drb_dense_batch_t P, void *stream);
+/* Failure detection (no counterpart in the reference).  Later launches of
+ * the plan limit every in-kernel wait to wait_ns nanoseconds (0 = the default,
+ * one second), and with stall_tile >= 0 the CTA of that output tile issues no
+ * loads, so its waits run out: the launch then stops early, leaves the
+ * unfinished tiles of Y unwritten and drb_dense_batch_check returns
+ * DRB_ERR_TIMEOUT; the plan stays usable.  stall_tile = -1 restores normal
+ * launches. */
+drb_status drb_dense_batch_set_wait(drb_dense_batch_t P, uint64_t wait_ns,
+                                    int32_t stall_tile);
 drb_status drb_dense_batch_destroy(drb_dense_batch_t P);
 
 /* out[0] = sum_i a[i]*b[i] (a == b gives the squared norm), f64 accumulation

@@ -6,8 +6,10 @@ drb.mp.distributed_sparse_matrix with a torch.distributed communicator and
 checks drb.mp.gemv -- root and no-root forms, one vector and a 20-wide
 slim matrix, csr_row and csr_eq -- against the oracle's restatement of the
 reference's per-rank loops and gather (oracle.gemv_row / gemv_eq with
-nseg = world size).  With --local oracle the per-rank product is the
-oracle's own loop (CPU ranks), so results must match bit for bit; with
+nseg = world size), and that a gemv with a root moves the partial results
+to the root alone (non-root ranks receive no bytes).  With --local oracle
+the per-rank product is the oracle's own loop (CPU ranks), so results must
+match bit for bit; with
 --local device it is this library's GPU kernel, checked within the
 reference tests' fp_equal tolerance.  The collectives run over gloo (host
 tensors; several ranks may then share one GPU, whose kernels never wait on
@@ -84,6 +86,10 @@ def run(rank, world, local):
                 want = ref(rp, ci, v, x, m, n, 1, oracle.ACC_T, world)
                 res = np.full(m, 7, v.dtype)
                 mp.gemv(root, res, a, b)
+                # the gather goes to the root alone (the reference's MPI_Gather)
+                got_bytes = a._sharded.last_gather_bytes
+                check(got_bytes == 0 if rank != root else got_bytes > 0 or world == 1,
+                      f"{tag}: root={root} gather bytes received {got_bytes}")
                 if rank == root:
                     if exact:
                         check(np.array_equal(res, want), f"{tag}: root={root} bits")
@@ -95,6 +101,8 @@ def run(rank, world, local):
                     check((res == 7).all(), f"{tag}: non-root result untouched")
                 res2 = np.zeros(m, v.dtype)
                 mp.gemv(res2, a, b)  # no root: the result on every rank
+                check(a._sharded.last_gather_bytes > 0 or world == 1,
+                      f"{tag}: no-root gather reaches every rank")
                 check(np.array_equal(res2, want) if exact else oracle.fp_equal(want, res2),
                       f"{tag}: no-root")
                 if "x_w20" in f:

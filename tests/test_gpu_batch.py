@@ -160,6 +160,20 @@ def test_batch_bf16_f32_x(mp):
     check_against_oracle(mats_np, xs, ys, 16, COL, 1e-5, round_bf16="v")
 
 
+@pytest.mark.parametrize("x_dtype", [None, torch.float32])
+def test_batch_bf16_sums_are_compensated(mp, x_dtype):
+    """BF16 storage sums two-sum compensated per block of four products (a
+    fused multiply-add chain per block, a two-sum into the row's sum): against
+    the long-double oracle on the bf16-rounded inputs the kernel read, a row's
+    error stays within 5u = 3.0e-7 of sum|a x| however long the row (the
+    batch holds one of 5000 nonzeros, where plain f32 sums drift by about
+    sqrt(5000) roundings)."""
+    mats_np = mixed_batch()
+    _, xs, ys, _ = run_batch(mp, mats_np, 16, COL, storage=torch.bfloat16, x_dtype=x_dtype)
+    check_against_oracle(mats_np, xs, ys, 16, COL, 5 * 2.0 ** -24,
+                         round_bf16="x" if x_dtype is None else "v")
+
+
 def test_batch_deterministic_rebind_and_launch_count(mp):
     """Two graph launches give identical bits; rebinding new x/y needs no new
     graph; each launch runs the pack and SpMM kernels (column-major)."""

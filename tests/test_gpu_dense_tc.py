@@ -100,6 +100,38 @@ def test_dense_tc_deterministic_and_launches(mp):
     P.destroy()
 
 
+def test_dense_tc_wait_timeout_is_reported_and_the_plan_recovers(mp):
+    """Failure detection without a fault: the CTA of one tile issues no loads
+    (drb_dense_batch_set_wait), so its pipeline wait runs out after 2 ms; the
+    kernel records DRB_ERR_TIMEOUT, the other CTAs stop at their next wait
+    after draining the copies they issued, and drb_dense_batch_check reports
+    it.  The next launch with normal waits gives oracle-correct results."""
+    from drb import _capi as capi
+    shapes = [(1000, 3000), (300, 257), (513, 777)]
+    As, xs, xcs, ys = [], [], [], []
+    for i, (m, n) in enumerate(shapes):
+        A, x, x_cm, y = make(m, n, 32, COL, 40 + i)
+        As.append(A), xs.append(x), xcs.append(x_cm), ys.append(y)
+    P = mp.dense_batch(As, xs, ys, 32, COL, ns=[n for _, n in shapes])
+    P.gemv()
+    P.check()
+    for tile in (0, 5):
+        P.set_wait(2_000_000, tile)
+        P.gemv()
+        with pytest.raises(capi.DrbError) as e:
+            P.check()
+        assert e.value.status == capi.DRB_ERR_TIMEOUT
+        P.check()  # the error word was cleared
+    P.set_wait()
+    for y in ys:
+        y.fill_(float("nan"))
+    P.gemv()
+    P.check()
+    for (m, n), A, x_cm, y in zip(shapes, As, xcs, ys):
+        check(y, A, x_cm, m, n, 32, COL)
+    P.destroy()
+
+
 def test_dense_tc_rejects(mp):
     from drb import _capi as capi
     A = torch.zeros(64, 100, device="cuda", dtype=torch.bfloat16)  # lda 100: not % 8
