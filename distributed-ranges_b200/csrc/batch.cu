@@ -218,14 +218,105 @@ __device__ __forceinline__ void two_sum_rn(float a, float b, float &s, float &e)
   e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
+// ---- packed f32 pairs (sm_100's f32x2 arithmetic) -------------------------
+// One instruction does the fma / add / sub / mul of two f32 elements, each
+// rounded exactly as its scalar form, so a lane's VEC sums take half the
+// issue slots (the BF16 kernel is bound by instruction issue).  The pair's
+// first element sits in the low 32 bits.
+__device__ __forceinline__ uint64_t pk2(float lo, float hi) {
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+  return d;
+}
+__device__ __forceinline__ void unpk2(uint64_t d, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(d));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+// Elements 2p and 2p+1 of a lane's VEC gathered X values as an f32 pair.
+template <class XT, int VEC>
+__device__ __forceinline__ uint64_t x_pair(const XWords<XT, VEC> &o, int p) {
+  if constexpr (sizeof(XT) == 4)
+    return pk2(__uint_as_float(o.w[2 * p]), __uint_as_float(o.w[2 * p + 1]));
+  else // one 32-bit word holds both bf16 values, the first in its low half
+    return pk2(__uint_as_float(o.w[p] << 16), __uint_as_float(o.w[p] & 0xffff0000u));
+}
+
 // The nonzeros [b, e) of one row staged at shared addresses colS/valS (byte
 // address of stage element 0), this lane's VEC sums (and, compensated, their
 // error terms cmp); the lane takes b, b + step, ... with kUnroll gathers in
-// flight.
+// flight.  f32 sums of an even VEC run on packed pairs.
 template <class V, class XT, int VEC, class A>
 __device__ __forceinline__ void row_sums(uint32_t colS, uint32_t valS, int b,
                                          int e, const XT *Xl, int ldx,
                                          int step, A (&acc)[VEC], A (&cmp)[VEC]) {
+  if constexpr (sizeof(A) == 4 && VEC % 2 == 0) {
+    constexpr int P = VEC / 2;
+    uint64_t a2[P], c2[P];
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      a2[p] = pk2(acc[2 * p], acc[2 * p + 1]);
+      c2[p] = pk2(cmp[2 * p], cmp[2 * p + 1]);
+    }
+    for (int q = b; q < e; q += kUnroll * step) {
+      XWords<XT, VEC> xv[kUnroll];
+      uint64_t v2[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; u++) {
+        const int qq = min(q + u * step, e - 1); // in range; extra lanes masked
+        const int32_t col = lds_s32(colS + 4 * qq);
+        const float v = to_acc(lds_val<V>(valS + (uint32_t)sizeof(V) * qq));
+        const float vm = q + u * step < e ? v : 0.0f;
+        v2[u] = pk2(vm, vm);
+        ldg_x<XT, VEC>(Xl + (int64_t)col * ldx, xv[u]);
+      }
+      if constexpr (Comp<V>::value) {
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+          uint64_t blk = mul2(v2[0], x_pair<XT, VEC>(xv[0], p));
+#pragma unroll
+          for (int u = 1; u < kUnroll; u++)
+            blk = fma2(v2[u], x_pair<XT, VEC>(xv[u], p), blk);
+          // two-sum of the pair: s + err == a2 + blk exactly
+          const uint64_t s = add2(a2[p], blk);
+          const uint64_t bb = sub2(s, a2[p]);
+          const uint64_t err = add2(sub2(a2[p], sub2(s, bb)), sub2(blk, bb));
+          a2[p] = s;
+          c2[p] = add2(c2[p], err);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++)
+#pragma unroll
+          for (int p = 0; p < P; p++)
+            a2[p] = fma2(v2[u], x_pair<XT, VEC>(xv[u], p), a2[p]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+      unpk2(a2[p], acc[2 * p], acc[2 * p + 1]);
+      unpk2(c2[p], cmp[2 * p], cmp[2 * p + 1]);
+    }
+    return;
+  }
   for (int q = b; q < e; q += kUnroll * step) {
     XWords<XT, VEC> xv[kUnroll];
     A vv[kUnroll];

@@ -349,6 +349,17 @@ drb_status drb_csr_create(drb_csr_t *out, int64_t m, int64_t n, int64_t nnz,
     if (A->tr)
       DRB_TRY(autotune_pipe(*A->tr, s, nullptr));
   }
+  // a column-blocked copy when x would not stay in L2 (after the autotuner,
+  // whose item variant it starts from)
+  DRB_TRY(colsplit_build(*A, s));
+  if (A->tr)
+    DRB_TRY(colsplit_build(*A->tr, s));
+  if (flags & DRB_FLAG_AUTOTUNE) {
+    DRB_TRY(colsplit_tune(*A, s));
+    if (A->tr)
+      DRB_TRY(colsplit_tune(*A->tr, s));
+  }
+  DRB_CUDA_TRY(cudaStreamSynchronize(s));
   *out = A.release();
   return DRB_OK;
 }
@@ -690,7 +701,10 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
   const size_t yb = (size_t)(A->storage == DRB_BF16 ? 4 : dtype_bytes(A->storage));
   DRB_TRY(A->xh_dev.ensure(xb * A->n * k));
   DRB_TRY(A->yh_dev.ensure(yb * A->m * k));
-  if (k == 1 && A->nnz >= kSegmentMinNnz && (A->pipe.nitems > 0 || A->sell.on))
+  // (a column-split handle runs its blocks in one go: y is then the same as
+  // drb_csr_gemv's, bit for bit)
+  if (k == 1 && A->nnz >= kSegmentMinNnz && (A->pipe.nitems > 0 || A->sell.on) &&
+      A->cblk.empty())
     return gemv_host_segmented(*A, x_host, y_host, xb, yb, s);
   if (A->n > 0)
     DRB_CUDA_TRY(cudaMemcpyAsync(A->xh_dev.p, x_host, xb * A->n * k,
@@ -742,6 +756,17 @@ drb_status drb_csr_variant(drb_csr_t A, int *variant) {
   return DRB_OK;
 }
 
+drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width) {
+  clear_error();
+  if (!A)
+    return invalid("A is NULL");
+  if (nblocks)
+    *nblocks = A->cblk.empty() ? 1 : (int)A->cblk.size();
+  if (block_width)
+    *block_width = A->cblk.empty() ? A->n : A->cbw;
+  return DRB_OK;
+}
+
 drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream) {
   clear_error();
   if (!A)
@@ -752,6 +777,9 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream) {
   DRB_TRY(autotune_pipe(*A, s, &v));
   if (A->tr)
     DRB_TRY(autotune_pipe(*A->tr, s, nullptr));
+  DRB_TRY(colsplit_tune(*A, s));
+  if (A->tr)
+    DRB_TRY(colsplit_tune(*A->tr, s));
   if (variant)
     *variant = v;
   return DRB_OK;
@@ -782,7 +810,11 @@ drb_status drb_csr_update_values(drb_csr_t A, const void *values,
                                (size_t)dtype_bytes(A->storage) * A->nnz,
                                cudaMemcpyDeviceToDevice, s));
   DRB_TRY(sell_pack_values(*A, s));
-  return adjoint_refresh_values(*A, s);
+  DRB_TRY(colsplit_refresh_values(*A, s));
+  DRB_TRY(adjoint_refresh_values(*A, s));
+  if (A->tr)
+    DRB_TRY(colsplit_refresh_values(*A->tr, s));
+  return DRB_OK;
 }
 
 drb_status drb_dense_gemv(int64_t m, int64_t n, const void *Am, int64_t lda,

@@ -152,10 +152,16 @@ struct PipePlan {
   std::vector<int64_t> seg_c0;      // first chunk of each segment (+ end)
   int64_t fin_c0 = 0, fin_c1 = -1;  // chunks the plain launch finishes (-1: all)
   uint64_t gen = 0; // bumped by every (re)build
+  // The plain launch adds its row sums to y instead of writing them (the
+  // second and later column blocks of a column-split handle, colsplit.cu).
+  bool accum = false;
 };
 
 drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
                            int rbytes, int group, int tile, int rows);
+// Elements per 16-byte vector group of a plan over values of vbytes and
+// column indices of cbytes.
+int plan_group(int vbytes, int cbytes);
 
 // rowptr buffers carry this many extra zeroed elements past rowptr[m] so a
 // 16-byte-rounded bulk copy of a rowptr slice stays inside the allocation.
@@ -220,6 +226,10 @@ struct Csr {
   int mrhs_layout = -1;
   // host copy of rowptr (int64), filled on first drb_csr_get_entries
   std::vector<int64_t> rowptr_h;
+  // column-blocked copy for the single-RHS gemv when x does not stay in L2
+  // (colsplit.cu): block b holds the nonzeros of columns [b*cbw, (b+1)*cbw)
+  std::vector<std::unique_ptr<Csr>> cblk;
+  int64_t cbw = 0;
   ~Csr();
 };
 
@@ -260,6 +270,13 @@ struct WarpResid;
 drb_status sell_launch(Csr &A, const void *x, void *y, const warpk::WarpResid *ra,
                        int64_t s0, int64_t s1, cudaStream_t s);
 drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen);
+// Column split (colsplit.cu): build A.cblk when x is too large for L2 (or
+// as DRB_COLSPLIT asks), refresh its values after A's change, run the
+// single-RHS gemv over it, and time its kernel variants.
+drb_status colsplit_build(Csr &A, cudaStream_t s);
+drb_status colsplit_refresh_values(Csr &A, cudaStream_t s);
+drb_status colsplit_launch(Csr &A, const void *x, void *y, cudaStream_t s);
+drb_status colsplit_tune(Csr &A, cudaStream_t s);
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
                        cudaStream_t s);
 drb_status residual_launch(Csr &A, const void *x, const void *b, void *y,
@@ -308,6 +325,11 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
   asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
+__device__ __forceinline__ uint64_t policy_evict_normal() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
 __device__ __forceinline__ uint64_t policy_evict_last() {
   uint64_t p;
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
@@ -322,6 +344,16 @@ __device__ __forceinline__ uint4 ld_stream16(const void *ptr, uint64_t pol) {
                : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
                : "l"(ptr), "l"(pol));
   return r;
+}
+
+// Store with an L2 eviction policy (results written once, e.g. y).
+__device__ __forceinline__ void st_hint(float *ptr, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(ptr), "f"(v), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st_hint(double *ptr, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(ptr), "d"(v), "l"(pol)
+               : "memory");
 }
 
 __device__ __forceinline__ float ld_keep(const float *ptr, uint64_t pol) {

@@ -13,8 +13,9 @@ namespace drb {
 using warpk::kRows;
 using warpk::WarpResid;
 
-// Kernel variant: item span 256 or 512 nonzeros, skewed or plain product
-// layout.  Encoded as tile | (skew ? 1 : 0) in build_pipe_plan's `tile`
+// Kernel variant: item span 128, 256 or 512 nonzeros, skewed or plain product
+// layout (128: 40-48 registers instead of 64, so 5-6 CTAs per SM instead of 4,
+// for storage whose 16-byte group is at most 4 elements).  Encoded as tile | (skew ? 1 : 0) in build_pipe_plan's `tile`
 // argument (0 = choose).  The choice does not change results beyond the
 // summation order of a chunked row, which is the same for both layouts.
 //
@@ -30,7 +31,7 @@ int choose_pipe_variant(int64_t, const void *, int) {
     const int t = std::atoi(e);
     const char *c = std::strchr(e, ',');
     const int sk = c ? std::atoi(c + 1) : 0;
-    if (t == 256 || t == 512)
+    if (t == 128 || t == 256 || t == 512)
       return t | (sk ? 1 : 0);
   }
   return 256 | 1;
@@ -43,7 +44,9 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
     tile = choose_pipe_variant(m, rowptr_host, rbytes);
   plan.skew = (tile & 1) != 0;
   tile &= ~1;
-  if (tile != 256 && tile != 512)
+  if (tile != 128 && tile != 256 && tile != 512)
+    tile = 256;
+  if (tile == 128 && group > 4) // a 128-nonzero item holds 32 groups of at most 4
     tile = 256;
   if (rows <= 0 || rows > kRows)
     rows = kRows;
@@ -210,7 +213,8 @@ drb_status rowdot_pipe_launch(Csr &A, const void *x, const void *w, void *y,
 
 int plan_group(int vbytes, int cbytes);
 
-// Times the four single-RHS row-block variants, and the sliced-ELL copy when
+// Times the single-RHS row-block variants (128-, 256- and 512-nonzero items,
+// skewed or plain layout; 128 only for 4-byte groups), and the sliced-ELL copy when
 // the matrix qualifies for one, on this matrix's sparsity pattern (x = 0,
 // three launches each after one warm-up) and keeps the fastest.  Returns the
 // chosen variant (tile | skew, or kVariantSell) in *chosen.
@@ -230,9 +234,15 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
   // the row-block variants, then the sliced-ELL copy when the rows allow one
   if (!A.sell.built)
     DRB_TRY(sell_build(A, rp.data(), A.rbytes, s));
-  const int variants[5] = {256 | 1, 256, 512 | 1, 512, kVariantSell};
-  const int nvar = A.sell.built ? 5 : 4;
-  float vms[5] = {3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f};
+  std::vector<int> variants = {256 | 1, 256, 512 | 1, 512};
+  if (group <= 4) { // 128-nonzero items: fewer registers, more warps per SM
+    variants.push_back(128 | 1);
+    variants.push_back(128);
+  }
+  if (A.sell.built)
+    variants.push_back(kVariantSell);
+  const int nvar = (int)variants.size();
+  std::vector<float> vms(nvar, 3.4e38f);
   drb_status st = DRB_OK;
   // Two rounds over the variants, each variant's best kept, after ~30 ms of
   // warm-up launches: a first variant timed while the clocks still ramp up

@@ -37,6 +37,8 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 
 #include "drb_internal.cuh"
 
@@ -186,8 +188,9 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
   const Chunk *__restrict__ chunks;
   Acc *partials;
   int *counters;
-  uint64_t pol_s, pol_x;
+  uint64_t pol_s, pol_x, pol_y;
   int lane;
+  int accum; // add the row sums to y (a later column block) instead of writing them
 
   __device__ __forceinline__ void fetch(S &sl, int64_t i) {
     sl.valid = i < nitems;
@@ -326,7 +329,8 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       }
       const Acc tot = group_sum(acc.s, acc.c, tpr);
       if (r < nrows && gl == 0) {
-        y[cur.r0 + r] = tot;
+        Acc *yp = y + cur.r0 + r;
+        ptx::st_hint(yp, accum ? *yp + tot : tot, pol_y);
         if (RESID) {
           if (dotw) {
             r2 += (double)tot * (double)bvec[cur.r0 + r];
@@ -348,7 +352,8 @@ __global__ void __launch_bounds__(kThreads)
               const V *__restrict__ vals, const XT *__restrict__ x,
               typename AccOf<V>::type *__restrict__ y, const Item *__restrict__ items,
               int64_t nitems, const Chunk *__restrict__ chunks,
-              typename AccOf<V>::type *partials, int *counters, WarpResid ra) {
+              typename AccOf<V>::type *partials, int *counters, WarpResid ra,
+              int ypol, int accum) {
   using Acc = typename AccOf<V>::type;
   __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
   __shared__ int s_rp[kWarps][kRows + 1];
@@ -356,10 +361,14 @@ __global__ void __launch_bounds__(kThreads)
   if (RESID && ra.stop && *static_cast<const volatile int *>(ra.stop))
     return; // uniform: every CTA reads the same word, written by an earlier launch
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // y is written once: evict-first by default so that it does not push the
+  // gathered x out of L2
   Kern<V, XT, CI, RI, TILE, SKEW, COMP> K{rowptr, colind, vals, x, y, items, nitems,
                                       chunks, partials, counters,
                                       ptx::policy_evict_first(), ptx::policy_evict_last(),
-                                      lane};
+                                      ypol ? ptx::policy_evict_normal()
+                                           : ptx::policy_evict_first(),
+                                      lane, accum};
   const Acc *bvec = static_cast<const Acc *>(ra.b);
   double r2 = 0.0;
   Acc *prod = s_prod[warp];
@@ -410,7 +419,8 @@ __global__ void __launch_bounds__(kThreads)
 // added in chunk order (the order of the ticketed finish).
 template <class Acc, bool COMP>
 __global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64_t c1,
-                             const Acc *__restrict__ partials, Acc *__restrict__ y) {
+                             const Acc *__restrict__ partials, Acc *__restrict__ y,
+                             int accum) {
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
   for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += nth) {
     const Chunk ch = chunks[c];
@@ -424,7 +434,7 @@ __global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64
       else
         sum.s += p;
     }
-    y[ch.row] = sum.value();
+    y[ch.row] = accum ? y[ch.row] + sum.value() : sum.value();
   }
 }
 
@@ -521,6 +531,16 @@ struct Shape {
   bool ready = false;
 };
 
+// L2 policy of the y stores: evict-first (0), or evict-normal (1) with
+// DRB_Y_STORE=normal, read once per process.
+inline int y_store_keep() {
+  static const int keep = [] {
+    const char *e = std::getenv("DRB_Y_STORE");
+    return (e && std::strcmp(e, "normal") == 0) ? 1 : 0;
+  }();
+  return keep;
+}
+
 template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP>
 drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
                        cudaStream_t s) {
@@ -542,10 +562,12 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
   if (ra)
     r = *ra;
   DRB_CUDA_TRY(cudaMemsetAsync(P.counters.p, 0, sizeof(unsigned), s)); // work counter
+  const int accum = (!RESID && P.accum) ? 1 : 0;
   kern<<<grid, kThreads, 0, s>>>(A.rowptr.as<RI>(), A.colind.as<CI>(), A.vals.as<V>(),
                                  static_cast<const XT *>(x), static_cast<Acc *>(y),
                                  P.items.as<Item>(), P.nitems, P.chunks.as<Chunk>(),
-                                 P.partials.as<Acc>(), P.counters.as<int>(), r);
+                                 P.partials.as<Acc>(), P.counters.as<int>(), r,
+                                 y_store_keep(), accum);
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
   if (RESID) {
@@ -565,7 +587,8 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
     if (c1 > c0) {
       const int g = (int)std::max<int64_t>(1, std::min<int64_t>(148 * 4, (c1 - c0 + 255) / 256));
       chunk_finish<Acc, COMP><<<g, 256, 0, s>>>(P.chunks.as<Chunk>(), c0, c1,
-                                                P.partials.as<Acc>(), static_cast<Acc *>(y));
+                                                P.partials.as<Acc>(), static_cast<Acc *>(y),
+                                                accum);
       note_launch();
       DRB_CUDA_TRY(cudaGetLastError());
     }
@@ -579,6 +602,11 @@ drb_status launch_variant(Csr &A, const void *x, void *y, const WarpResid *ra,
   if (A.pipe.nitems == 0)
     return DRB_OK;
   const bool sk = A.pipe.skew;
+  if constexpr (Slot<V, CI, 256>::G * 32 <= 128) {
+    if (A.pipe.tile == 128)
+      return sk ? launch_tile<V, XT, CI, RI, 128, true, RESID, COMP>(A, x, y, ra, s)
+                : launch_tile<V, XT, CI, RI, 128, false, RESID, COMP>(A, x, y, ra, s);
+  }
   if (A.pipe.tile == 512)
     return sk ? launch_tile<V, XT, CI, RI, 512, true, RESID, COMP>(A, x, y, ra, s)
               : launch_tile<V, XT, CI, RI, 512, false, RESID, COMP>(A, x, y, ra, s);

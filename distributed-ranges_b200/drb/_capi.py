@@ -95,6 +95,7 @@ DRB_SYMBOLS = [
     ("drb_csr_check", _st, [_vp, _vp]),
     ("drb_csr_variant", _st, [_vp, C.POINTER(_i32)]),
     ("drb_csr_autotune", _st, [_vp, C.POINTER(_i32), _vp]),
+    ("drb_csr_column_blocks", _st, [_vp, C.POINTER(_i32), C.POINTER(_i64)]),
     ("drb_csr_residual_norm2", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("drb_csr_gemv_backward", _st, [_vp, _vp, _vp, _vp, _vp, _vp]),
     ("drb_csr_update_values", _st, [_vp, _vp, _vp]),

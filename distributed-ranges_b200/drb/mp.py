@@ -412,11 +412,18 @@ class distributed_sparse_matrix:
                                          int(k), layout, _stream(stream)))
 
     def variant(self) -> int:
-        """Single-RHS kernel variant: item span (256/512) | 1 if skewed, or
+        """Single-RHS kernel variant: item span (128/256/512) | 1 if skewed, or
         2048 for the sliced-ELL copy (short, regular rows)."""
         v = C.c_int()
         check(capi.lib.drb_csr_variant(self._h, C.byref(v)))
         return v.value
+
+    def column_blocks(self):
+        """(blocks, block width) of the single-RHS product's column split
+        (drb_csr_column_blocks): (1, n) when x stays in L2."""
+        nb, bw = C.c_int(), C.c_int64()
+        check(capi.lib.drb_csr_column_blocks(self._h, C.byref(nb), C.byref(bw)))
+        return nb.value, bw.value
 
     def autotune(self, stream=None) -> int:
         """Time the kernel variants on this sparsity pattern, keep the best."""

@@ -160,8 +160,8 @@ drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
 drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
                              int64_t k, drb_layout layout, void *stream);
 
-/* Kernel variant of the single right-hand-side product: item span (256 or
- * 512 nonzeros) | 1 when the skewed (bank-conflict-free) product layout is
+/* Kernel variant of the single right-hand-side product: item span (128, 256
+ * or 512 nonzeros) | 1 when the skewed (bank-conflict-free) product layout is
  * used, or 2048 for the sliced-ELL copy (slices of 32 rows padded to their
  * longest row, lane = row), which drb_csr_create takes by default when the
  * longest row has <= 64 nonzeros, padding adds <= 20% and twice the copy's
@@ -173,6 +173,21 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
  * variants up to the summation order inside a row. */
 drb_status drb_csr_variant(drb_csr_t A, int *variant);
 drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
+
+/* Column blocks of the single right-hand-side product (no counterpart in the
+ * reference; a layout choice inside the handle).  A randomly gathered x stays
+ * in B200's L2 only up to about 48 MB, so drb_csr_create regroups the
+ * nonzeros of an F32/F64 handle whose x is larger than 64 MiB (and that
+ * reuses x at least twice, nnz >= 2n) into *nblocks column blocks of
+ * *block_width columns (x slices of at most 48 MiB), kept as a second copy
+ * of the values and column indices on the device, when that copy fits with
+ * 1 GB to spare.  gemv (k = 1, device or host pointers) then runs one launch
+ * per block, adding the blocks' row sums in block order: deterministic, the
+ * same bits from drb_csr_gemv and drb_csr_gemv_host.  The adjoint's
+ * transposed matrix is split the same way.  The environment variable
+ * DRB_COLSPLIT=<n> (read when a handle is created) asks for n blocks (0 or 1:
+ * none).  *nblocks = 1 (and *block_width = n) when the handle is not split. */
+drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width);
 
 /* Synchronise `stream` and report device-side failures of earlier launches
  * on this handle: DRB_ERR_TIMEOUT when a bounded in-kernel wait expired (the

@@ -1,0 +1,128 @@
+"""The column-blocked single-RHS plan (csrc/colsplit.cu) against the oracle.
+
+drb_csr_create regroups a handle's nonzeros by column block when x is too
+large to stay in L2 (above 64 MiB); DRB_COLSPLIT=<n>, read at creation,
+forces n blocks on the small matrices used here.  Each case checks the
+split product against the oracle's long-double csr_row loop (FP32 within
+1e-5, FP64 within 1e-12 of sum |a x| per row), determinism, the host-pointer
+call (bit-identical to the device call), a value update, and the adjoint
+whose transposed matrix is split as well."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mp():
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from drb import mp as _mp
+    return _mp
+
+
+def rel_err(y, y_ref, denom):
+    d = np.maximum(np.asarray(denom, np.float64), np.finfo(np.float64).tiny)
+    return float(np.max(np.abs(np.asarray(y, np.float64) - y_ref) / d)) if len(d) else 0.0
+
+
+def mixed_rows(dtype, unsorted, seed=3):
+    """Empty, short, long and chunked rows (longer than one 512-nonzero item,
+    and one of 70,001 nonzeros), columns uniform over 300,000; with
+    `unsorted` each row's columns are shuffled."""
+    rng = np.random.default_rng(seed)
+    n = 300_000
+    lens = np.concatenate([rng.integers(0, 40, 4000), [0, 1, 2047, 2049, 0],
+                           [70_001], rng.integers(0, 6, 2000), rng.integers(100, 2000, 100)])
+    m = len(lens)
+    rp = np.zeros(m + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.empty(rp[-1], np.int32)
+    for r in range(m):
+        if lens[r]:
+            c = rng.choice(n, lens[r], replace=False)
+            ci[rp[r]:rp[r + 1]] = c if unsorted else np.sort(c)
+    v = rng.uniform(-1, 1, rp[-1]).astype(dtype)
+    return rp.astype(np.int32), ci, v, m, n
+
+
+def check(y, rp, ci, v, x, m, n, tol):
+    y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
+    assert rel_err(y, y64, oracle.absdot(rp, ci, v, x, m, n)) <= tol
+
+
+@pytest.mark.parametrize("unsorted", [False, True])
+@pytest.mark.parametrize("nblk", [2, 3, 8])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_split_gemv_parity(mp, dtype, nblk, unsorted, monkeypatch):
+    monkeypatch.setenv("DRB_COLSPLIT", str(nblk))
+    rp, ci, v, m, n = mixed_rows(dtype, unsorted)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    nb, bw = a.column_blocks()
+    assert nb == nblk and bw == -(-n // nblk)
+    x = np.random.default_rng(7).uniform(-1, 1, n).astype(dtype)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.full((m,), float("nan"), dtype=xt.dtype, device="cuda")
+    a.gemv_device(xt, yt)
+    a.check()
+    y1 = yt.cpu().numpy()
+    check(y1, rp, ci, v, x, m, n, tol)
+    for _ in range(2):  # repeat launches: same bits
+        a.gemv_device(xt, yt)
+    assert np.array_equal(yt.cpu().numpy().view(np.uint8), y1.view(np.uint8))
+    yh = np.empty(m, dtype)
+    a.gemv_host(x, yh)  # host pointers: the same blocks, the same bits
+    assert np.array_equal(yh.view(np.uint8), y1.view(np.uint8))
+    # new values reach the blocks' copy
+    v2 = (np.random.default_rng(8).uniform(-1, 1, len(v))).astype(dtype)
+    a.update_values(torch.from_numpy(v2).cuda())
+    a.gemv_device(xt, yt)
+    check(yt.cpu().numpy(), rp, ci, v2, x, m, n, tol)
+    a.destroy()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_split_matches_unsplit_within_tolerance(mp, dtype, monkeypatch):
+    """The same handle without a split (DRB_COLSPLIT=0): both within the gate
+    of the oracle, and the unsplit one reports one block."""
+    rp, ci, v, m, n = mixed_rows(dtype, False, seed=11)
+    x = np.random.default_rng(12).uniform(-1, 1, n).astype(dtype)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    out = {}
+    for nb in ("0", "4"):
+        monkeypatch.setenv("DRB_COLSPLIT", nb)
+        a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0,
+                                         autotune=True)
+        assert a.column_blocks()[0] == (1 if nb == "0" else 4)
+        xt = torch.from_numpy(x).cuda()
+        yt = torch.empty(m, dtype=xt.dtype, device="cuda")
+        a.gemv_device(xt, yt)
+        out[nb] = yt.cpu().numpy()
+        check(out[nb], rp, ci, v, x, m, n, tol)
+        a.destroy()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_split_adjoint(mp, dtype, monkeypatch):
+    """x-bar = A^T y-bar on the split transposed matrix, against the oracle's
+    csr_row loop on the explicit transpose; a-bar unchanged by the split."""
+    monkeypatch.setenv("DRB_COLSPLIT", "3")
+    rp, ci, v, m, n = mixed_rows(dtype, False, seed=21)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0, adjoint=True)
+    yb = np.random.default_rng(22).uniform(-1, 1, m).astype(dtype)
+    x = np.random.default_rng(23).uniform(-1, 1, n).astype(dtype)
+    xbar = torch.empty(n, dtype=torch.from_numpy(x).dtype, device="cuda")
+    abar = torch.empty(len(v), dtype=xbar.dtype, device="cuda")
+    mp.gemv_backward(a, torch.from_numpy(yb).cuda(), torch.from_numpy(x).cuda(), xbar, abar)
+    a.check()
+    cp, ri, vt = oracle.transpose(rp, ci, v, m, n)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    check(xbar.cpu().numpy(), cp, ri, vt, yb, n, m, tol)
+    ab_ref = oracle.abar(rp, ci, yb, x, m)
+    assert np.allclose(abar.cpu().numpy(), ab_ref, rtol=1e-6 if dtype == np.float32 else 1e-15,
+                       atol=0)
+    a.destroy()

@@ -211,7 +211,7 @@ def test_autotune_variants_agree(mp, dtype):
     tol = 1e-5 if dtype == np.float32 else 1e-12
     a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0,
                                      adjoint=True, autotune=True)
-    assert a.variant() in (256, 257, 512, 513)
+    assert a.variant() in (128, 129, 256, 257, 512, 513)
     xt = torch.from_numpy(x).cuda()
     yt = torch.empty(m, dtype=xt.dtype, device="cuda")
     a.gemv_device(xt, yt)
@@ -223,16 +223,25 @@ def test_autotune_variants_agree(mp, dtype):
     assert rel_err(yt.cpu().numpy(), y64, d) <= tol
 
 
-@pytest.mark.parametrize("variant", ["256,0", "256,1", "512,0", "512,1"])
-def test_each_variant_parity(mp, variant, monkeypatch):
+@pytest.mark.parametrize("variant", ["128,0", "128,1", "256,0", "256,1", "512,0", "512,1"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_each_variant_parity(mp, variant, dtype, monkeypatch):
     monkeypatch.setenv("DRB_SPMV_VARIANT", variant)
-    rp, ci, v, m, n = chunky_matrix(np.float32)
-    x = np.random.default_rng(13).uniform(-1, 1, n).astype(np.float32)
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    x = np.random.default_rng(13).uniform(-1, 1, n).astype(dtype)
     a, y = gpu_gemv(mp, rp, ci, v, m, n, x)
     t, sk = (int(s) for s in variant.split(","))
     assert a.variant() == (t | sk)
     y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
-    assert rel_err(y, y64, oracle.absdot(rp, ci, v, x, m, n)) <= 1e-5
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert rel_err(y, y64, oracle.absdot(rp, ci, v, x, m, n)) <= tol
+    # the fused residual on the same variant
+    b = np.random.default_rng(14).uniform(-1, 1, m).astype(dtype)
+    bt = torch.from_numpy(b).cuda()
+    yt = torch.empty(m, dtype=bt.dtype, device="cuda")
+    r2 = float(mp.residual_norm2(a, torch.from_numpy(x).cuda(), bt, yt))
+    ref = float(np.sum((y64 - b.astype(np.float64)) ** 2))
+    assert abs(r2 - ref) <= 1e-4 * ref
 
 
 @pytest.mark.parametrize("keep64", [False, True])
