@@ -1188,11 +1188,19 @@ def profile_case(name):
       residual4m  the fused ||Ax - b||^2 on that matrix (same variant);
       adjoint_lap_f32  gemv_backward (xbar and abar) on the 2048^2 5-point
                Laplacian, FP32, random values;
-      dot_f32  the dot kernel on two FP32 vectors of 2^26 elements (2 x 256 MB)."""
+      dot_f32  the dot kernel on two FP32 vectors of 2^26 elements (2 x 256 MB);
+      probe4m  the streaming-gather probe on the powerlaw4m matrix (column
+               indices and values streamed, x gathered; the SpMV's floor);
+      colsplit_f64_4m  the FP64 SpMV on 4,194,304 rows of the bench
+               distribution with 16,777,216 columns (x 128 MB): three column
+               blocks, one launch each;
+      spmm_k16_4m  k = 16 column-major on the powerlaw4m matrix (X 1.07 GB);
+      batch16_bf16  the batched SpMM of batch16 with BF16 storage and X
+               (compensated sums)."""
     import torch
     import drb
     from drb import mp
-    if name == "batch16":
+    if name in ("batch16", "batch16_bf16"):
         k = BATCH_K
         rng = np.random.default_rng(SEED + 5)
         rows = rng.integers(1024, 200001, size=BATCH_COUNT)[:16]
@@ -1201,9 +1209,11 @@ def profile_case(name):
         for i, m in enumerate(rows):
             m = int(m)
             rp, ci, v = drb.gen.uniform_rows_csr(m, m, lo=8, hi=64, seed=SEED + 1000 + i)
+            kw = dict(storage=torch.bfloat16) if name == "batch16_bf16" else {}
             mats.append(mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, m)), 0,
-                                                     distr=mp.csr_row_distribution))
-            xs.append(torch.empty(m * k, device="cuda").uniform_(-1, 1, generator=g))
+                                                     distr=mp.csr_row_distribution, **kw))
+            xv = torch.empty(m * k, device="cuda").uniform_(-1, 1, generator=g)
+            xs.append(xv.to(torch.bfloat16) if kw else xv)
             ys.append(torch.empty(m * k, device="cuda"))
         b = mp.batch(mats, k, 0)
         b.bind(xs, ys)
@@ -1257,6 +1267,33 @@ def profile_case(name):
         mp.conjugate_gradient(A, b, x, max_iters=8, rtol=0.0)
         x.zero_()
         mp.conjugate_gradient(A, b, x, max_iters=24, rtol=0.0)
+    elif name in ("probe4m", "colsplit_f64_4m", "spmm_k16_4m"):
+        alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
+        rp, ci, v = drb.gen.powerlaw_csr(4_194_304, N_COLS, alpha=alpha, hi=ZIPF_HI,
+                                         seed=SEED)
+        dt = np.float64 if name == "colsplit_f64_4m" else np.float32
+        if name == "probe4m":
+            os.environ["DRB_SPMV_VARIANT"] = "256,1"
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v.astype(dt), rp, ci,
+                                                            (4_194_304, N_COLS)),
+                                         0, distr=mp.csr_row_distribution)
+        x = torch.from_numpy(drb.gen.values(N_COLS, seed=SEED + 1).astype(dt)).cuda()
+        if name == "probe4m":
+            import drb_probe
+            for _ in range(4):
+                drb_probe.gather_probe(A, x)
+        elif name == "colsplit_f64_4m":
+            assert A.column_blocks()[0] == 3, A.column_blocks()
+            y = torch.empty(4_194_304, device="cuda", dtype=torch.float64)
+            for _ in range(4):
+                A.gemv_device(x, y)
+        else:
+            k = 16
+            X = torch.empty(N_COLS * k, device="cuda").uniform_(-1, 1)
+            Y = torch.empty(4_194_304 * k, device="cuda")
+            for _ in range(4):
+                A.gemv_device(X, Y, k)
+        A.check()
     elif name in ("powerlaw4m", "residual4m"):
         os.environ["DRB_SPMV_VARIANT"] = "256,0"
         alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
@@ -1317,9 +1354,10 @@ def main():
                     help="rows of the power-law matrix (profiling a smaller case)")
     ap.add_argument("--cols", type=int, default=N_COLS,
                     help="columns (keep 16777216 to keep the 64 MB x footprint)")
-    ap.add_argument("--profile-case", choices=["batch16", "dense64", "dense_f32", "laplacian_f64",
-                                               "cg_f64", "powerlaw4m", "residual4m", "dot_f32",
-                                               "adjoint_lap_f32"],
+    ap.add_argument("--profile-case", choices=["batch16", "batch16_bf16", "dense64", "dense_f32",
+                                               "laplacian_f64", "cg_f64", "powerlaw4m",
+                                               "residual4m", "dot_f32", "adjoint_lap_f32",
+                                               "probe4m", "colsplit_f64_4m", "spmm_k16_4m"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
