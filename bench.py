@@ -259,6 +259,14 @@ def run_reference(args):
     return 0
 
 
+def kernel_name(variant):
+    """The single-RHS kernel behind a drb_csr_variant code."""
+    if variant == 2048:
+        return "sell_spmv<float,int>"
+    name = "spmv_warp_pipe" if variant & 2 else "spmv_warp"
+    return "%s<float,int,int,%d,%d>" % (name, variant & ~3, variant & 1)
+
+
 def workload_config(alpha, nnz):
     name = ("csr_powerlaw_16M_fp32" if (M, N_COLS) == (16_777_216, 16_777_216)
             else f"csr_powerlaw_{M}x{N_COLS}_fp32")
@@ -410,7 +418,7 @@ def run_ours(args):
                          "frac": round(achieved / peak, 4),
                          "traffic": (profiled_traffic("spmv_warp_powerlaw16M_fp32")
                                      if (M, N_COLS) == (16_777_216, 16_777_216) else None),
-                         "kernel": "spmv_warp<float,int,int,%d,%d>" % (variant & ~1, variant & 1),
+                         "kernel": kernel_name(variant),
                          "gather_ceiling": {
                              "what": "random x gathers: ~1 L1->crossbar request per SM per "
                                      "clock (288 G/s measured on this B200)",

@@ -752,7 +752,8 @@ drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
 drb_status drb_csr_variant(drb_csr_t A, int *variant) {
   if (!A || !variant)
     return invalid("NULL argument");
-  *variant = A->sell.on ? kVariantSell : A->pipe.tile | (A->pipe.skew ? 1 : 0);
+  *variant = A->sell.on ? kVariantSell
+                        : A->pipe.tile | (A->pipe.skew ? 1 : 0) | (A->pipe.two_slot ? 2 : 0);
   return DRB_OK;
 }
 

@@ -264,7 +264,7 @@ drb_status colsplit_build(Csr &A, cudaStream_t s) {
   if (nblk < 2)
     return DRB_OK;
   // the blocks' rows are shorter than A's (about 1/nblk of each row)
-  const int tile = A.pipe.tile | (A.pipe.skew ? 1 : 0);
+  const int tile = A.pipe.tile | (A.pipe.skew ? 1 : 0) | (A.pipe.two_slot ? 2 : 0);
   return A.storage == DRB_F64 ? build_v<double>(A, nblk, tile, s)
                               : build_v<float>(A, nblk, tile, s);
 }
@@ -289,10 +289,11 @@ drb_status colsplit_tune(Csr &A, cudaStream_t s) {
     return DRB_OK;
   const int vb = dtype_bytes(A.storage);
   const int group = plan_group(vb, A.cbytes);
-  std::vector<int> variants = {256 | 1, 256};
+  std::vector<int> variants = {256 | 1, 256, 256 | 3};
   if (group <= 4) {
     variants.push_back(128 | 1);
     variants.push_back(128);
+    variants.push_back(128 | 3);
   }
   DevBuf xb, yb;
   DRB_TRY(xb.alloc((size_t)vb * (A.n + 1)));

@@ -137,6 +137,7 @@ static_assert(sizeof(Item) == 32, "Item is 32 bytes");
 struct PipePlan {
   int tile = 0, rows = 0, group = 0;
   bool skew = false; // skewed product layout in the row reduction
+  bool two_slot = false; // the pipelined kernel (spmv_warp_pipe) for plain products
   int64_t nitems = 0, nchunks = 0, nsplit = 0;
   DevBuf items;    // Item[nitems]
   DevBuf chunks;   // Chunk[nchunks]

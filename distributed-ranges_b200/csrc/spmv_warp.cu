@@ -15,7 +15,8 @@ using warpk::WarpResid;
 
 // Kernel variant: item span 128, 256 or 512 nonzeros, skewed or plain product
 // layout (128: 40-48 registers instead of 64, so 5-6 CTAs per SM instead of 4,
-// for storage whose 16-byte group is at most 4 elements).  Encoded as tile | (skew ? 1 : 0) in build_pipe_plan's `tile`
+// for storage whose 16-byte group is at most 4 elements), and | 2 for the
+// two-slot pipelined kernel of the plain product (128 or 256, skewed).  Encoded as tile | (skew ? 1 : 0) in build_pipe_plan's `tile`
 // argument (0 = choose).  The choice does not change results beyond the
 // summation order of a chunked row, which is the same for both layouts.
 //
@@ -25,14 +26,17 @@ using warpk::WarpResid;
 // power-law: 1.61 ms against 1.97 ms for 512-nonzero items) once chunked
 // rows finish in a separate pass.  The environment variable
 // DRB_SPMV_VARIANT="tile,skew" (e.g. "512,0") overrides it for handles
-// created afterwards; drb_csr_autotune measures all four instead.
+// created afterwards ("128,1,1": the two-slot kernel); drb_csr_autotune
+// measures them all instead.
 int choose_pipe_variant(int64_t, const void *, int) {
   if (const char *e = std::getenv("DRB_SPMV_VARIANT")) {
     const int t = std::atoi(e);
     const char *c = std::strchr(e, ',');
     const int sk = c ? std::atoi(c + 1) : 0;
+    const char *c2 = c ? std::strchr(c + 1, ',') : nullptr;
+    const int two = c2 ? std::atoi(c2 + 1) : 0;
     if (t == 128 || t == 256 || t == 512)
-      return t | (sk ? 1 : 0);
+      return t | (sk ? 1 : 0) | (two ? 2 : 0);
   }
   return 256 | 1;
 }
@@ -43,11 +47,17 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
   if (tile == 0)
     tile = choose_pipe_variant(m, rowptr_host, rbytes);
   plan.skew = (tile & 1) != 0;
-  tile &= ~1;
+  plan.two_slot = (tile & 2) != 0;
+  tile &= ~3;
   if (tile != 128 && tile != 256 && tile != 512)
     tile = 256;
   if (tile == 128 && group > 4) // a 128-nonzero item holds 32 groups of at most 4
     tile = 256;
+  if (plan.two_slot) {
+    plan.skew = true; // the pipelined kernel uses the skewed layout only
+    if (tile == 512)
+      plan.two_slot = false;
+  }
   if (rows <= 0 || rows > kRows)
     rows = kRows;
   plan.tile = tile;
@@ -234,10 +244,11 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
   // the row-block variants, then the sliced-ELL copy when the rows allow one
   if (!A.sell.built)
     DRB_TRY(sell_build(A, rp.data(), A.rbytes, s));
-  std::vector<int> variants = {256 | 1, 256, 512 | 1, 512};
+  std::vector<int> variants = {256 | 1, 256, 512 | 1, 512, 256 | 3};
   if (group <= 4) { // 128-nonzero items: fewer registers, more warps per SM
     variants.push_back(128 | 1);
     variants.push_back(128);
+    variants.push_back(128 | 3);
   }
   if (A.sell.built)
     variants.push_back(kVariantSell);

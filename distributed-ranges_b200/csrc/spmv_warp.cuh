@@ -344,6 +344,113 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     __syncwarp(); // the shared slice is rewritten by the next item
   }
 
+  // ---- the two-slot pipelined form (spmv_warp_pipe) --------------------------
+  // Issues the x gathers of the item in `sl` (zeros where masked, or for an
+  // empty slot) into xg.
+  __device__ __forceinline__ void gather(const S &sl, Acc (&xg)[NG][G]) {
+    const int off = sl.valid ? (int)(sl.d.p0 - sl.a0) : 0;
+    const int end = sl.valid ? off + sl.d.len : 0;
+    const int ng = (end + G - 1) / G;
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        const int q = g * G + i;
+        xg[j][i] = (g < ng && q >= off && q < end) ? ld_x(x + sl.c[j][i], pol_x) : Acc(0);
+      }
+    }
+  }
+
+  // Runs the item in `cur`, whose x values are in xg; meanwhile issues the
+  // gathers of `nxt` (loaded one step earlier) into xg and refills `cur`
+  // with item `refill`, so a warp keeps one item's gathers in flight while it
+  // sums the previous item's rows.
+  __device__ __forceinline__ void step(S &cur, const S &nxt, Acc (&xg)[NG][G],
+                                       int64_t refill, Acc *prod, int *srp) {
+    const Item it = cur.d;
+    const int off = (int)(it.p0 - cur.a0), end = off + it.len;
+    const int ng = (end + G - 1) / G;
+    if (it.nrows == 0) {
+      CSum<Acc> acc;
+#pragma unroll
+      for (int j = 0; j < NG; j++) {
+        const int g = lane + 32 * j;
+#pragma unroll
+        for (int i = 0; i < G; i++) {
+          const int q = g * G + i;
+          if (g < ng && q >= off && q < end) {
+            const Acc p = to_acc(cur.v[j][i]) * xg[j][i];
+            if (COMP)
+              acc.add(p);
+            else
+              acc.s += p;
+          }
+        }
+      }
+      gather(nxt, xg);
+      fetch(cur, refill);
+      const Acc tot = group_sum(acc.s, acc.c, 32);
+      if (lane == 0)
+        partials[it.chunk] = tot; // the row is completed by the finish pass
+      return;
+    }
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+      if (g < ng) {
+        if (SKEW) {
+#pragma unroll
+          for (int i = 0; i < G; i++)
+            prod[skew(g * G + i)] = to_acc(cur.v[j][i]) * xg[j][i];
+        } else {
+          constexpr int PER = 16 / sizeof(Acc);
+#pragma unroll
+          for (int h = 0; h < G / PER; h++) {
+            Vec16<Acc> w;
+#pragma unroll
+            for (int i = 0; i < PER; i++)
+              w.t[i] = to_acc(cur.v[j][h * PER + i]) * xg[j][h * PER + i];
+            *reinterpret_cast<uint4 *>(prod + g * G + h * PER) = w.u;
+          }
+        }
+      }
+    }
+    if (lane <= it.nrows)
+      srp[lane] = cur.rp0;
+    if (lane + 32 <= it.nrows)
+      srp[lane + 32] = cur.rp1;
+    if (lane == 0 && 64 <= it.nrows)
+      srp[64] = cur.rp2;
+    __syncwarp();
+    gather(nxt, xg);    // the next item's gathers fly while these rows are summed
+    fetch(cur, refill); // and the item after it streams in
+    const int nrows = it.nrows;
+    int tpr = 1;
+    while (tpr < 32 && tpr * 2 * nrows <= 32)
+      tpr <<= 1;
+    const int groups = 32 / tpr, gid = lane / tpr, gl = lane & (tpr - 1);
+    for (int base = 0; base < nrows; base += groups) {
+      const int r = base + gid;
+      CSum<Acc> acc;
+      if (r < nrows) {
+        const int b = srp[r], e = srp[r + 1];
+        for (int q = b + gl; q < e; q += tpr) {
+          const Acc p = prod[SKEW ? skew(q) : q];
+          if (COMP)
+            acc.add(p);
+          else
+            acc.s += p;
+        }
+      }
+      const Acc tot = group_sum(acc.s, acc.c, tpr);
+      if (r < nrows && gl == 0) {
+        Acc *yp = y + it.r0 + r;
+        ptx::st_hint(yp, accum ? *yp + tot : tot, pol_y);
+      }
+    }
+    __syncwarp(); // the shared slice is rewritten by the next item
+  }
 };
 
 template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP>
@@ -412,6 +519,60 @@ __global__ void __launch_bounds__(kThreads)
     }
     cur = next;
     next = advance();
+  }
+}
+
+// The plain product (no fused reduction) with two item slots per warp: the
+// gathers of item t+1 are issued before the rows of item t are summed, and
+// item t+2's indices and values load meanwhile, so each item exposes one
+// memory latency instead of two (gathers waiting on the indices they need).
+// Same items, work counter, products and sums as spmv_warp: the same bits.
+template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
+__global__ void __launch_bounds__(kThreads, TILE == 128 ? 4 : 2)
+    spmv_warp_pipe(const RI *__restrict__ rowptr, const CI *__restrict__ colind,
+                   const V *__restrict__ vals, const XT *__restrict__ x,
+                   typename AccOf<V>::type *__restrict__ y, const Item *__restrict__ items,
+                   int64_t nitems, const Chunk *__restrict__ chunks,
+                   typename AccOf<V>::type *partials, int *counters, WarpResid,
+                   int ypol, int accum) {
+  using Acc = typename AccOf<V>::type;
+  using Kt = Kern<V, XT, CI, RI, TILE, SKEW, COMP>;
+  __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
+  __shared__ int s_rp[kWarps][kRows + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  Kt K{rowptr, colind, vals, x, y, items, nitems, chunks, partials, counters,
+       ptx::policy_evict_first(), ptx::policy_evict_last(),
+       ypol ? ptx::policy_evict_normal() : ptx::policy_evict_first(), lane, accum};
+  Acc *prod = s_prod[warp];
+  int *srp = s_rp[warp];
+  constexpr int kBatch = 8; // items per grab, as spmv_warp
+  auto grab = [&]() -> int64_t {
+    unsigned v = 0;
+    if (lane == 0)
+      v = atomicAdd(reinterpret_cast<unsigned *>(counters), (unsigned)kBatch);
+    return (int64_t)__shfl_sync(0xffffffffu, v, 0);
+  };
+  int64_t base = grab();
+  int k = 0;
+  auto advance = [&]() -> int64_t {
+    if (++k == kBatch) {
+      base = grab();
+      k = 0;
+    }
+    return base + k;
+  };
+  Slot<V, CI, TILE> A, B;
+  Acc xg[Kt::NG][Kt::G];
+  K.fetch(A, base);
+  K.fetch(B, advance());
+  K.gather(A, xg);
+  // a warp's item indices only grow, so once a slot comes back empty every
+  // later one would too
+  while (A.valid) {
+    K.step(A, B, xg, advance(), prod, srp);
+    if (!B.valid)
+      break;
+    K.step(B, A, xg, advance(), prod, srp);
   }
 }
 
@@ -541,13 +702,19 @@ inline int y_store_keep() {
   return keep;
 }
 
-template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP>
+template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool RESID, bool COMP,
+          bool PIPE = false>
 drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
                        cudaStream_t s) {
   using Acc = typename AccOf<V>::type;
   PipePlan &P = A.pipe;
   static Shape shape[64];
-  auto kern = spmv_warp<V, XT, CI, RI, TILE, SKEW, RESID, COMP>;
+  auto kern = [] {
+    if constexpr (PIPE)
+      return spmv_warp_pipe<V, XT, CI, RI, TILE, SKEW, COMP>;
+    else
+      return spmv_warp<V, XT, CI, RI, TILE, SKEW, RESID, COMP>;
+  }();
   const int dev = A.device < 64 ? A.device : 0;
   if (!shape[dev].ready) {
     int occ = 0, sms = 0;
@@ -602,6 +769,15 @@ drb_status launch_variant(Csr &A, const void *x, void *y, const WarpResid *ra,
   if (A.pipe.nitems == 0)
     return DRB_OK;
   const bool sk = A.pipe.skew;
+  if constexpr (!RESID) {
+    if (A.pipe.two_slot) { // the pipelined kernel: skewed layout, 128 or 256 nonzeros
+      if constexpr (Slot<V, CI, 256>::G * 32 <= 128) {
+        if (A.pipe.tile == 128)
+          return launch_tile<V, XT, CI, RI, 128, true, false, COMP, true>(A, x, y, ra, s);
+      }
+      return launch_tile<V, XT, CI, RI, 256, true, false, COMP, true>(A, x, y, ra, s);
+    }
+  }
   if constexpr (Slot<V, CI, 256>::G * 32 <= 128) {
     if (A.pipe.tile == 128)
       return sk ? launch_tile<V, XT, CI, RI, 128, true, RESID, COMP>(A, x, y, ra, s)

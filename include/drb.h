@@ -161,7 +161,9 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
                              int64_t k, drb_layout layout, void *stream);
 
 /* Kernel variant of the single right-hand-side product: item span (128, 256
- * or 512 nonzeros) | 1 when the skewed (bank-conflict-free) product layout is
+ * or 512 nonzeros) | 2 for the two-slot pipelined kernel (the next item's
+ * gathers in flight while the current item's rows are summed; 128 or 256,
+ * skewed) | 1 when the skewed (bank-conflict-free) product layout is
  * used, or 2048 for the sliced-ELL copy (slices of 32 rows padded to their
  * longest row, lane = row), which drb_csr_create takes by default when the
  * longest row has <= 64 nonzeros, padding adds <= 20% and twice the copy's

@@ -211,7 +211,7 @@ def test_autotune_variants_agree(mp, dtype):
     tol = 1e-5 if dtype == np.float32 else 1e-12
     a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0,
                                      adjoint=True, autotune=True)
-    assert a.variant() in (128, 129, 256, 257, 512, 513)
+    assert a.variant() in (128, 129, 131, 256, 257, 259, 512, 513)
     xt = torch.from_numpy(x).cuda()
     yt = torch.empty(m, dtype=xt.dtype, device="cuda")
     a.gemv_device(xt, yt)
@@ -223,15 +223,20 @@ def test_autotune_variants_agree(mp, dtype):
     assert rel_err(yt.cpu().numpy(), y64, d) <= tol
 
 
-@pytest.mark.parametrize("variant", ["128,0", "128,1", "256,0", "256,1", "512,0", "512,1"])
+@pytest.mark.parametrize("variant", ["128,0", "128,1", "256,0", "256,1", "512,0", "512,1",
+                                     "128,1,1", "256,1,1"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_each_variant_parity(mp, variant, dtype, monkeypatch):
+    """Every item span and layout, and the two-slot pipelined kernel ("t,1,1"),
+    within the gate of the oracle, with the fused residual on the same plan
+    (the residual keeps the one-slot kernel)."""
     monkeypatch.setenv("DRB_SPMV_VARIANT", variant)
     rp, ci, v, m, n = chunky_matrix(dtype)
     x = np.random.default_rng(13).uniform(-1, 1, n).astype(dtype)
     a, y = gpu_gemv(mp, rp, ci, v, m, n, x)
-    t, sk = (int(s) for s in variant.split(","))
-    assert a.variant() == (t | sk)
+    parts = [int(s) for s in variant.split(",")] + [0]
+    t, sk, two = parts[0], parts[1], parts[2]
+    assert a.variant() == (t | sk | (2 if two else 0))
     y64 = oracle.gemv_row(rp, ci, v, x, m, n, 1, oracle.ACC_LD)
     tol = 1e-5 if dtype == np.float32 else 1e-12
     assert rel_err(y, y64, oracle.absdot(rp, ci, v, x, m, n)) <= tol
@@ -242,6 +247,10 @@ def test_each_variant_parity(mp, variant, dtype, monkeypatch):
     r2 = float(mp.residual_norm2(a, torch.from_numpy(x).cuda(), bt, yt))
     ref = float(np.sum((y64 - b.astype(np.float64)) ** 2))
     assert abs(r2 - ref) <= 1e-4 * ref
+    if two:  # the pipelined kernel gives the same bits as the one-slot kernel
+        monkeypatch.setenv("DRB_SPMV_VARIANT", f"{t},1")
+        _, y1 = gpu_gemv(mp, rp, ci, v, m, n, x)
+        assert np.array_equal(y.view(np.uint8), y1.view(np.uint8))
 
 
 @pytest.mark.parametrize("keep64", [False, True])
