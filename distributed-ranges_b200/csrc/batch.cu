@@ -251,6 +251,15 @@ __device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+// d = a * b + c for bf16 a and b (bits) and f32 c, one rounding: the bf16
+// product is exact in f32, so this is fmaf(float(a), float(b), c) without
+// unpacking the bf16 operands first.
+__device__ __forceinline__ float fma_bf16(uint16_t a, uint16_t b, float c) {
+  float d;
+  asm("fma.rn.f32.bf16 %0, %1, %2, %3;" : "=f"(d) : "h"(a), "h"(b), "f"(c));
+  return d;
+}
+
 // Elements 2p and 2p+1 of a lane's VEC gathered X values as an f32 pair.
 template <class XT, int VEC>
 __device__ __forceinline__ uint64_t x_pair(const XWords<XT, VEC> &o, int p) {
@@ -276,19 +285,45 @@ __device__ __forceinline__ void row_sums(uint32_t colS, uint32_t valS, int b,
       a2[p] = pk2(acc[2 * p], acc[2 * p + 1]);
       c2[p] = pk2(cmp[2 * p], cmp[2 * p + 1]);
     }
+    // bf16 values and bf16 X: the block's chains run on the bf16 operands
+    constexpr bool kMixed = Comp<V>::value && sizeof(XT) == 2;
     for (int q = b; q < e; q += kUnroll * step) {
       XWords<XT, VEC> xv[kUnroll];
       uint64_t v2[kUnroll];
+      uint16_t vb[kUnroll];
 #pragma unroll
       for (int u = 0; u < kUnroll; u++) {
         const int qq = min(q + u * step, e - 1); // in range; extra lanes masked
         const int32_t col = lds_s32(colS + 4 * qq);
-        const float v = to_acc(lds_val<V>(valS + (uint32_t)sizeof(V) * qq));
-        const float vm = q + u * step < e ? v : 0.0f;
-        v2[u] = pk2(vm, vm);
+        const V raw = lds_val<V>(valS + (uint32_t)sizeof(V) * qq);
+        const bool in = q + u * step < e;
+        if constexpr (kMixed) {
+          vb[u] = in ? (uint16_t)raw : (uint16_t)0; // bf16 +0 for masked lanes
+        } else {
+          const float vm = in ? to_acc(raw) : 0.0f;
+          v2[u] = pk2(vm, vm);
+        }
         ldg_x<XT, VEC>(Xl + (int64_t)col * ldx, xv[u]);
       }
-      if constexpr (Comp<V>::value) {
+      if constexpr (kMixed) {
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+          // one 32-bit word holds right-hand sides 2p (low half) and 2p+1
+          float lo = fma_bf16(vb[0], (uint16_t)(xv[0].w[p] & 0xffffu), 0.0f);
+          float hi = fma_bf16(vb[0], (uint16_t)(xv[0].w[p] >> 16), 0.0f);
+#pragma unroll
+          for (int u = 1; u < kUnroll; u++) {
+            lo = fma_bf16(vb[u], (uint16_t)(xv[u].w[p] & 0xffffu), lo);
+            hi = fma_bf16(vb[u], (uint16_t)(xv[u].w[p] >> 16), hi);
+          }
+          const uint64_t blk = pk2(lo, hi);
+          const uint64_t s = add2(a2[p], blk);
+          const uint64_t bb = sub2(s, a2[p]);
+          const uint64_t err = add2(sub2(a2[p], sub2(s, bb)), sub2(blk, bb));
+          a2[p] = s;
+          c2[p] = add2(c2[p], err);
+        }
+      } else if constexpr (Comp<V>::value) {
 #pragma unroll
         for (int p = 0; p < P; p++) {
           uint64_t blk = mul2(v2[0], x_pair<XT, VEC>(xv[0], p));
