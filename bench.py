@@ -230,6 +230,14 @@ def cpu_reference(rp, ci, v, x, steps, warmup, budget_s=None):
     return nth, times
 
 
+def cpu_spread(bytes_, times):
+    """GB/s of the slowest, median and fastest pass: the host is shared, so its
+    figure moves from run to run."""
+    gb = sorted(bytes_ / t / 1e9 for t in times)
+    return {"min": round(gb[0], 3), "median": round(statistics.median(gb), 3),
+            "max": round(gb[-1], 3), "passes": len(gb)}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -251,7 +259,8 @@ def run_reference(args):
         "cpu_baseline": {"value": round(val, 3), "unit": "GB/s", "cores": nth, "kind": "port",
                          "sample": f"{len(times)} full passes over the matrix (csr_row CPU "
                                    f"loop of csr_row_distribution.hpp:116-133, {nth} threads "
-                                   f"= {nth} ranks, local phase + gather)"},
+                                   f"= {nth} ranks, local phase + gather)",
+                         "spread": cpu_spread(bytes_, times)},
         "e2e": {"value": round(val, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -405,7 +414,8 @@ def run_ours(args):
             cpu = {"value": round(bytes_ / tc / 1e9, 3), "unit": "GB/s", "cores": nth,
                    "kind": "port",
                    "sample": f"{len(times)} full passes over the same matrix with the "
-                             f"restated csr_row CPU loop, {nth} threads (median)"}
+                             f"restated csr_row CPU loop, {nth} threads (median)",
+                   "spread": cpu_spread(bytes_, times)}
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms, 4),
@@ -502,14 +512,15 @@ def extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes32, fwd_ms, stream):
 
     # FP64 SpMV on the same pattern
     A64 = mp.distributed_sparse_matrix(mp.csr_matrix_view(v.astype(np.float64), rp, ci,
-                                                          (M, N_COLS)), 0)
+                                                          (M, N_COLS)), 0, autotune=True)
     x64 = xd.double()
     y64 = torch.empty(M, dtype=torch.float64, device="cuda")
     A64.gemv_device(x64, y64)
     ms = statistics.mean(timed_launches(lambda: A64.gemv_device(x64, y64), steps, stream))
     b64 = alg_bytes(M, N_COLS, nnz, 8, 4, 4, 8, 8)
     out["spmv_fp64"] = {"ms": round(ms, 4), "GBps": round(b64 / (ms * 1e-3) / 1e9, 2),
-                        "frac": round(b64 / (ms * 1e-3) / 1e9 / peak, 4)}
+                        "frac": round(b64 / (ms * 1e-3) / 1e9 / peak, 4),
+                        "column_blocks": A64.column_blocks()[0]}
     if not args.no_parity:
         import oracle
         record_parity("spmv_fp64", oracle.csr_check(rp, ci, v.astype(np.float64), x.astype(
@@ -1190,9 +1201,10 @@ def profile_case(name):
                (4,194,304 rows, FP64 values, int32 indices; 335 MB);
       cg_f64   conjugate gradients on that Laplacian, FP64: one warm-up solve
                of 8 iterations, then 24 iterations (rtol 0);
-      powerlaw4m  the bench's SpMV kernel variant (256-nonzero items, plain
-               product layout) on the first 4,194,304 rows' worth of the bench
-               distribution (16,777,216 columns, so the same 64 MB x);
+      powerlaw4m  the SpMV kernel variant of DRB_SPMV_VARIANT (default 256,0:
+               256-nonzero items, plain product layout) on the first 4,194,304
+               rows' worth of the bench distribution (16,777,216 columns, so the
+               same 64 MB x);
       residual4m  the fused ||Ax - b||^2 on that matrix (same variant);
       adjoint_lap_f32  gemv_backward (xbar and abar) on the 2048^2 5-point
                Laplacian, FP32, random values;
@@ -1303,7 +1315,7 @@ def profile_case(name):
                 A.gemv_device(X, Y, k)
         A.check()
     elif name in ("powerlaw4m", "residual4m"):
-        os.environ["DRB_SPMV_VARIANT"] = "256,0"
+        os.environ.setdefault("DRB_SPMV_VARIANT", "256,0")  # or the variant asked for
         alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
         rp, ci, v = drb.gen.powerlaw_csr(4_194_304, N_COLS, alpha=alpha, hi=ZIPF_HI,
                                          seed=SEED)

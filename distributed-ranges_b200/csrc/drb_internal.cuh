@@ -153,9 +153,6 @@ struct PipePlan {
   std::vector<int64_t> seg_c0;      // first chunk of each segment (+ end)
   int64_t fin_c0 = 0, fin_c1 = -1;  // chunks the plain launch finishes (-1: all)
   uint64_t gen = 0; // bumped by every (re)build
-  // The plain launch adds its row sums to y instead of writing them (the
-  // second and later column blocks of a column-split handle, colsplit.cu).
-  bool accum = false;
 };
 
 drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
@@ -228,8 +225,12 @@ struct Csr {
   // host copy of rowptr (int64), filled on first drb_csr_get_entries
   std::vector<int64_t> rowptr_h;
   // column-blocked copy for the single-RHS gemv when x does not stay in L2
-  // (colsplit.cu): block b holds the nonzeros of columns [b*cbw, (b+1)*cbw)
-  std::vector<std::unique_ptr<Csr>> cblk;
+  // (colsplit.cu): a virtual CSR whose row b*(m+1) + r holds row r's nonzeros
+  // of columns [b*cbw, (b+1)*cbw), its block-major partial sums and the block
+  // count (0: no split)
+  std::unique_ptr<Csr> csplit;
+  DevBuf csplit_y;
+  int csplit_nblk = 0;
   int64_t cbw = 0;
   ~Csr();
 };
@@ -271,7 +272,7 @@ struct WarpResid;
 drb_status sell_launch(Csr &A, const void *x, void *y, const warpk::WarpResid *ra,
                        int64_t s0, int64_t s1, cudaStream_t s);
 drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen);
-// Column split (colsplit.cu): build A.cblk when x is too large for L2 (or
+// Column split (colsplit.cu): build A.csplit when x is too large for L2 (or
 // as DRB_COLSPLIT asks), refresh its values after A's change, run the
 // single-RHS gemv over it, and time its kernel variants.
 drb_status colsplit_build(Csr &A, cudaStream_t s);

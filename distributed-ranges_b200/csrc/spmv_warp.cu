@@ -283,15 +283,21 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen) {
         break;
       if ((st = spmv_pipe_launch(A, xb.p, yb.p, s)) != DRB_OK)
         break;
-      cudaEventRecord(e0, s);
-      for (int i = 0; i < 3 && st == DRB_OK; i++)
+      // the fastest of five separately timed launches: variants differ by a
+      // few percent, less than the spread of a sum of launches
+      for (int i = 0; i < 5 && st == DRB_OK; i++) {
+        cudaEventRecord(e0, s);
         st = spmv_pipe_launch(A, xb.p, yb.p, s);
-      cudaEventRecord(e1, s);
-      if (st != DRB_OK || cudaEventSynchronize(e1) != cudaSuccess)
-        break;
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      vms[iv] = std::min(vms[iv], ms);
+        cudaEventRecord(e1, s);
+        float ms = 0.f;
+        if (st != DRB_OK || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+          if (st == DRB_OK)
+            st = DRB_ERR_CUDA;
+          break;
+        }
+        vms[iv] = std::min(vms[iv], ms);
+      }
     }
   }
   int best = variants[0], best_rb = variants[0];

@@ -190,7 +190,6 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
   int *counters;
   uint64_t pol_s, pol_x, pol_y;
   int lane;
-  int accum; // add the row sums to y (a later column block) instead of writing them
 
   __device__ __forceinline__ void fetch(S &sl, int64_t i) {
     sl.valid = i < nitems;
@@ -329,8 +328,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       }
       const Acc tot = group_sum(acc.s, acc.c, tpr);
       if (r < nrows && gl == 0) {
-        Acc *yp = y + cur.r0 + r;
-        ptx::st_hint(yp, accum ? *yp + tot : tot, pol_y);
+        ptx::st_hint(y + cur.r0 + r, tot, pol_y);
         if (RESID) {
           if (dotw) {
             r2 += (double)tot * (double)bvec[cur.r0 + r];
@@ -445,8 +443,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
       }
       const Acc tot = group_sum(acc.s, acc.c, tpr);
       if (r < nrows && gl == 0) {
-        Acc *yp = y + it.r0 + r;
-        ptx::st_hint(yp, accum ? *yp + tot : tot, pol_y);
+        ptx::st_hint(y + it.r0 + r, tot, pol_y);
       }
     }
     __syncwarp(); // the shared slice is rewritten by the next item
@@ -460,7 +457,7 @@ __global__ void __launch_bounds__(kThreads)
               typename AccOf<V>::type *__restrict__ y, const Item *__restrict__ items,
               int64_t nitems, const Chunk *__restrict__ chunks,
               typename AccOf<V>::type *partials, int *counters, WarpResid ra,
-              int ypol, int accum) {
+              int ypol) {
   using Acc = typename AccOf<V>::type;
   __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
   __shared__ int s_rp[kWarps][kRows + 1];
@@ -475,7 +472,7 @@ __global__ void __launch_bounds__(kThreads)
                                       ptx::policy_evict_first(), ptx::policy_evict_last(),
                                       ypol ? ptx::policy_evict_normal()
                                            : ptx::policy_evict_first(),
-                                      lane, accum};
+                                      lane};
   const Acc *bvec = static_cast<const Acc *>(ra.b);
   double r2 = 0.0;
   Acc *prod = s_prod[warp];
@@ -534,7 +531,7 @@ __global__ void __launch_bounds__(kThreads, TILE == 128 ? 4 : 2)
                    typename AccOf<V>::type *__restrict__ y, const Item *__restrict__ items,
                    int64_t nitems, const Chunk *__restrict__ chunks,
                    typename AccOf<V>::type *partials, int *counters, WarpResid,
-                   int ypol, int accum) {
+                   int ypol) {
   using Acc = typename AccOf<V>::type;
   using Kt = Kern<V, XT, CI, RI, TILE, SKEW, COMP>;
   __shared__ __align__(16) Acc s_prod[kWarps][TILE + TILE / 32];
@@ -542,7 +539,7 @@ __global__ void __launch_bounds__(kThreads, TILE == 128 ? 4 : 2)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   Kt K{rowptr, colind, vals, x, y, items, nitems, chunks, partials, counters,
        ptx::policy_evict_first(), ptx::policy_evict_last(),
-       ypol ? ptx::policy_evict_normal() : ptx::policy_evict_first(), lane, accum};
+       ypol ? ptx::policy_evict_normal() : ptx::policy_evict_first(), lane};
   Acc *prod = s_prod[warp];
   int *srp = s_rp[warp];
   constexpr int kBatch = 8; // items per grab, as spmv_warp
@@ -580,8 +577,7 @@ __global__ void __launch_bounds__(kThreads, TILE == 128 ? 4 : 2)
 // added in chunk order (the order of the ticketed finish).
 template <class Acc, bool COMP>
 __global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64_t c1,
-                             const Acc *__restrict__ partials, Acc *__restrict__ y,
-                             int accum) {
+                             const Acc *__restrict__ partials, Acc *__restrict__ y) {
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
   for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += nth) {
     const Chunk ch = chunks[c];
@@ -595,7 +591,7 @@ __global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64
       else
         sum.s += p;
     }
-    y[ch.row] = accum ? y[ch.row] + sum.value() : sum.value();
+    y[ch.row] = sum.value();
   }
 }
 
@@ -729,12 +725,11 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
   if (ra)
     r = *ra;
   DRB_CUDA_TRY(cudaMemsetAsync(P.counters.p, 0, sizeof(unsigned), s)); // work counter
-  const int accum = (!RESID && P.accum) ? 1 : 0;
   kern<<<grid, kThreads, 0, s>>>(A.rowptr.as<RI>(), A.colind.as<CI>(), A.vals.as<V>(),
                                  static_cast<const XT *>(x), static_cast<Acc *>(y),
                                  P.items.as<Item>(), P.nitems, P.chunks.as<Chunk>(),
                                  P.partials.as<Acc>(), P.counters.as<int>(), r,
-                                 y_store_keep(), accum);
+                                 y_store_keep());
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
   if (RESID) {
@@ -754,8 +749,7 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
     if (c1 > c0) {
       const int g = (int)std::max<int64_t>(1, std::min<int64_t>(148 * 4, (c1 - c0 + 255) / 256));
       chunk_finish<Acc, COMP><<<g, 256, 0, s>>>(P.chunks.as<Chunk>(), c0, c1,
-                                                P.partials.as<Acc>(), static_cast<Acc *>(y),
-                                                accum);
+                                                P.partials.as<Acc>(), static_cast<Acc *>(y));
       note_launch();
       DRB_CUDA_TRY(cudaGetLastError());
     }

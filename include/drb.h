@@ -182,9 +182,12 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
  * nonzeros of an F32/F64 handle whose x is larger than 64 MiB (and that
  * reuses x at least twice, nnz >= 2n) into *nblocks column blocks of
  * *block_width columns (x slices of at most 48 MiB), kept as a second copy
- * of the values and column indices on the device, when that copy fits with
- * 1 GB to spare.  gemv (k = 1, device or host pointers) then runs one launch
- * per block, adding the blocks' row sums in block order: deterministic, the
+ * of the values and column indices on the device (block-major: every row's
+ * nonzeros of block 0, then of block 1, ...), with nblocks partial sums per
+ * row of scratch, when that fits with 1 GB to spare.  gemv (k = 1, device or
+ * host pointers) then runs one launch over the copy -- its warps move through
+ * the blocks in order, so one x slice at a time is hot in L2 -- and a short
+ * pass that adds each row's block sums in block order: deterministic, the
  * same bits from drb_csr_gemv and drb_csr_gemv_host.  The adjoint's
  * transposed matrix is split the same way.  The environment variable
  * DRB_COLSPLIT=<n> (read when a handle is created) asks for n blocks (0 or 1:
