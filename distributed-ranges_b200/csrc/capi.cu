@@ -704,7 +704,7 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
   // (a column-split handle runs its blocks in one go: y is then the same as
   // drb_csr_gemv's, bit for bit)
   if (k == 1 && A->nnz >= kSegmentMinNnz && (A->pipe.nitems > 0 || A->sell.on) &&
-      !A->csplit)
+      (!A->csplit || A->sell.on))
     return gemv_host_segmented(*A, x_host, y_host, xb, yb, s);
   if (A->n > 0)
     DRB_CUDA_TRY(cudaMemcpyAsync(A->xh_dev.p, x_host, xb * A->n * k,
@@ -762,9 +762,9 @@ drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width
   if (!A)
     return invalid("A is NULL");
   if (nblocks)
-    *nblocks = A->csplit ? A->csplit_nblk : 1;
+    *nblocks = (A->csplit && !A->sell.on) ? A->csplit_nblk : 1;
   if (block_width)
-    *block_width = A->csplit ? A->cbw : A->n;
+    *block_width = (A->csplit && !A->sell.on) ? A->cbw : A->n;
   return DRB_OK;
 }
 

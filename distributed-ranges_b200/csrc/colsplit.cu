@@ -154,6 +154,8 @@ unsigned flat_grid(int64_t n) {
 int split_blocks(const Csr &A) {
   if (A.storage != DRB_F32 && A.storage != DRB_F64)
     return 0;
+  if (A.sell.on) // short regular rows (a stencil): the sliced-ELL kernel's gathers are local
+    return 0;
   if (A.m == 0 || A.n < 2 || A.nnz == 0)
     return 0;
   if (const char *e = std::getenv("DRB_COLSPLIT")) {

@@ -290,7 +290,8 @@ drb_status build_plan(Plan &plan, int64_t m, const void *rowptr_host,
 drb_status spmv_launch(Csr &A, const void *x, void *y, int64_t k,
                        drb_layout layout, cudaStream_t s) {
   if (k == 1)
-    return A.csplit ? colsplit_launch(A, x, y, s) : spmv_pipe_launch(A, x, y, s);
+    return (A.csplit && !A.sell.on) ? colsplit_launch(A, x, y, s)
+                                    : spmv_pipe_launch(A, x, y, s);
   // k > 1: the batched SpMM kernel on a batch of this one handle (2.0-2.3x
   // the row-block kernel below at k = 2..20 on 4M-row and 16.8M-row
   // matrices); the row-block kernel covers what a batch does not take

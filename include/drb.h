@@ -191,7 +191,9 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
  * same bits from drb_csr_gemv and drb_csr_gemv_host.  The adjoint's
  * transposed matrix is split the same way.  The environment variable
  * DRB_COLSPLIT=<n> (read when a handle is created) asks for n blocks (0 or 1:
- * none).  *nblocks = 1 (and *block_width = n) when the handle is not split. */
+ * none).  A handle on its sliced-ELL copy (short regular rows, whose gathers
+ * are local) is not split.  *nblocks = 1 (and *block_width = n) when the
+ * handle is not split. */
 drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width);
 
 /* Synchronise `stream` and report device-side failures of earlier launches

@@ -126,3 +126,20 @@ def test_split_adjoint(mp, dtype, monkeypatch):
     assert np.allclose(abar.cpu().numpy(), ab_ref, rtol=1e-6 if dtype == np.float32 else 1e-15,
                        atol=0)
     a.destroy()
+
+
+def test_stencil_stays_on_sliced_ell(mp, monkeypatch):
+    """A 5-point Laplacian (short regular rows, local gathers) keeps its
+    sliced-ELL copy and is not split, even when a split is asked for."""
+    import drb
+    monkeypatch.setenv("DRB_COLSPLIT", "3")
+    rp, ci, v = drb.gen.laplacian2d_csr(256, value_dtype=np.float64)
+    rp = rp.astype(np.int32)
+    m = len(rp) - 1
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, m)), 0)
+    assert a.variant() == 2048 and a.column_blocks() == (1, m)
+    x = np.random.default_rng(31).uniform(-1, 1, m)
+    y = torch.empty(m, dtype=torch.float64, device="cuda")
+    a.gemv_device(torch.from_numpy(x).cuda(), y)
+    check(y.cpu().numpy(), rp, ci, v, x, m, m, 1e-12)
+    a.destroy()
