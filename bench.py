@@ -436,6 +436,7 @@ def run_ours(args):
                          "traffic": (profiled_traffic("spmv_warp_powerlaw16M_fp32")
                                      if (M, N_COLS) == (16_777_216, 16_777_216) else None),
                          "kernel": kernel_name(variant),
+                         "column_blocks": A.column_blocks()[0],
                          "gather_ceiling": {
                              "what": "random x gathers: ~1 L1->crossbar request per SM per "
                                      "clock (288 G/s measured on this B200)",
@@ -1211,7 +1212,9 @@ def profile_case(name):
       powerlaw4m  the SpMV kernel variant of DRB_SPMV_VARIANT (default 256,0:
                256-nonzero items, plain product layout) on the first 4,194,304
                rows' worth of the bench distribution (16,777,216 columns, so the
-               same 64 MB x);
+               same 64 MB x, in two column blocks like the bench's handle: one
+               spmv_warp launch over the block-major copy, chunk_finish and
+               split_combine; DRB_COLSPLIT=0 for the unsplit product);
       residual4m  the fused ||Ax - b||^2 on that matrix (same variant);
       adjoint_lap_f32  gemv_backward (xbar and abar) on the 2048^2 5-point
                Laplacian, FP32, random values;
@@ -1220,7 +1223,7 @@ def profile_case(name):
                indices and values streamed, x gathered; the SpMV's floor);
       colsplit_f64_4m  the FP64 SpMV on 4,194,304 rows of the bench
                distribution with 16,777,216 columns (x 128 MB): three column
-               blocks, one launch each;
+               blocks in one launch, then split_combine;
       spmm_k16_4m  k = 16 column-major on the powerlaw4m matrix (X 1.07 GB);
       batch16_bf16  the batched SpMM of batch16 with BF16 storage and X
                (compensated sums)."""

@@ -701,10 +701,11 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
   const size_t yb = (size_t)(A->storage == DRB_BF16 ? 4 : dtype_bytes(A->storage));
   DRB_TRY(A->xh_dev.ensure(xb * A->n * k));
   DRB_TRY(A->yh_dev.ensure(yb * A->m * k));
-  // (a column-split handle runs its blocks in one go: y is then the same as
+  // (both pipelines run the device call's items and sums: y is the same as
   // drb_csr_gemv's, bit for bit)
-  if (k == 1 && A->nnz >= kSegmentMinNnz && (A->pipe.nitems > 0 || A->sell.on) &&
-      (!A->csplit || A->sell.on))
+  if (k == 1 && A->csplit && !A->sell.on)
+    return colsplit_gemv_host(*A, x_host, y_host, xb, yb, s);
+  if (k == 1 && A->nnz >= kSegmentMinNnz && (A->pipe.nitems > 0 || A->sell.on))
     return gemv_host_segmented(*A, x_host, y_host, xb, yb, s);
   if (A->n > 0)
     DRB_CUDA_TRY(cudaMemcpyAsync(A->xh_dev.p, x_host, xb * A->n * k,
@@ -764,7 +765,7 @@ drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width
   if (nblocks)
     *nblocks = (A->csplit && !A->sell.on) ? A->csplit_nblk : 1;
   if (block_width)
-    *block_width = (A->csplit && !A->sell.on) ? A->cbw : A->n;
+    *block_width = (A->csplit && !A->sell.on) ? A->cbounds[1] - A->cbounds[0] : A->n;
   return DRB_OK;
 }
 

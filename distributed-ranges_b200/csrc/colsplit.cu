@@ -10,19 +10,29 @@
 // So when x is larger than kSplitAbove, the handle keeps a second copy of its
 // nonzeros grouped by column block, as one "virtual" CSR matrix: its row
 // b*(m+1) + r holds the nonzeros of row r whose columns lie in block b
-// ([b*bw, (b+1)*bw), columns kept global, each row's order kept), and its
+// ([c_b, c_{b+1}), columns kept global, each row's order kept), and its
 // rows b*(m+1) + m are empty separators.  The unchanged persistent SpMV runs
 // over it in ONE launch into a block-major scratch y; its work counter hands
 // out items in order, so at any time nearly all warps work inside one block
 // and only that block's slice of x is hot in L2.  A last small pass adds the
 // blocks' row sums into y in block order (deterministic).  The scratch costs
-// nblk * (m + 1) partial sums, written once and read once.
+// nblk * (m + 1) partial sums, written once and read once.  Measured on that
+// pattern: FP32 (x = 64 MB) 1.470 ms in two blocks against 1.525 ms unsplit,
+// FP64 (x = 128 MB) 1.90 ms in three blocks against 3.57 ms.
 //
 // The regrouping runs on the device at plan time: a warp per row counts its
 // nonzeros per block with ballots, a scan per block gives the blocks' row
 // starts (offset by the blocks before them), and a second warp-per-row pass
 // scatters the nonzeros (a ballot per block gives each lane its place), so
 // rows need not be sorted.
+//
+// The host-pointer gemv (colsplit_gemv_host) pipelines over the blocks: x
+// goes up slice by slice on a copy stream, each block's items start as soon
+// as its slice is on the device, and the last block runs in row segments
+// whose combined rows copy back while the next segments compute -- so most of
+// the SpMV hides behind x's upload and most of y's download behind the last
+// block.  The segments run the same items, chunk sums and combine as the one
+// launch: y is bit-identical to the device-pointer call.
 #include <algorithm>
 #include <cstdlib>
 #include <vector>
@@ -35,15 +45,25 @@ namespace drb {
 namespace {
 
 constexpr int kMaxBlocks = 8;
-constexpr int64_t kSplitAbove = 64ll << 20; // split when x is larger than this
+constexpr int64_t kSplitAbove = 48ll << 20; // split when x is larger than this
 constexpr int64_t kSplitBlock = 48ll << 20; // and give each block at most this
 
 struct BlockOffsets {
   int64_t off[kMaxBlocks]; // first nonzero of each block in the regrouped arrays
 };
 
-__device__ __forceinline__ int block_of(int64_t col, int64_t bw, int nblk) {
-  return (int)min(col / bw, (int64_t)nblk - 1);
+// First column of each block (c[0] = 0); blocks past nblk unused.
+struct Bounds {
+  int64_t c[kMaxBlocks];
+  int nblk;
+};
+
+__device__ __forceinline__ int block_of(int64_t col, const Bounds &B) {
+  int b = 0;
+#pragma unroll
+  for (int j = 1; j < kMaxBlocks; j++)
+    b += (j < B.nblk && col >= B.c[j]) ? 1 : 0;
+  return b;
 }
 
 // cnt[b * (m + 1) + r] = nonzeros of row r in column block b (a warp per row);
@@ -51,7 +71,8 @@ __device__ __forceinline__ int block_of(int64_t col, int64_t bw, int nblk) {
 template <class CI, class RI>
 __global__ void __launch_bounds__(256)
     split_count(const RI *__restrict__ rp, const CI *__restrict__ ci, int64_t m,
-                int64_t bw, int nblk, RI *__restrict__ cnt) {
+                Bounds B, RI *__restrict__ cnt) {
+  const int nblk = B.nblk;
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
@@ -62,7 +83,7 @@ __global__ void __launch_bounds__(256)
       c[bb] = 0;
     for (int64_t base = p0; base < p1; base += 32) {
       const int64_t p = base + lane;
-      const int b = p < p1 ? block_of((int64_t)ci[p], bw, nblk) : -1;
+      const int b = p < p1 ? block_of((int64_t)ci[p], B) : -1;
 #pragma unroll
       for (int bb = 0; bb < kMaxBlocks; bb++)
         if (bb < nblk)
@@ -91,8 +112,9 @@ __global__ void split_offsets(RI *__restrict__ rp, int64_t m, int nblk, BlockOff
 template <class CI, class RI, class V>
 __global__ void __launch_bounds__(256)
     split_scatter(const RI *__restrict__ rp, const CI *__restrict__ ci,
-                  const V *__restrict__ v, int64_t m, int64_t bw, int nblk,
+                  const V *__restrict__ v, int64_t m, Bounds B,
                   const RI *__restrict__ rpv, CI *__restrict__ civ, V *__restrict__ vv) {
+  const int nblk = B.nblk;
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -109,7 +131,7 @@ __global__ void __launch_bounds__(256)
       const bool on = p < p1;
       const CI col = on ? ci[p] : CI(0);
       const V val = on ? v[p] : V(0);
-      const int b = on ? block_of((int64_t)col, bw, nblk) : -1;
+      const int b = on ? block_of((int64_t)col, B) : -1;
 #pragma unroll
       for (int bb = 0; bb < kMaxBlocks; bb++) {
         if (bb < nblk) {
@@ -127,11 +149,11 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// y[r] = sum over blocks b (in order) of ys[b * (m + 1) + r].
+// y[r] = sum over blocks b (in order) of ys[b * (m + 1) + r], rows [r0, r1).
 template <class Acc>
 __global__ void split_combine(const Acc *__restrict__ ys, Acc *__restrict__ y, int64_t m,
-                              int nblk) {
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+                              int64_t r0, int64_t r1, int nblk) {
+  for (int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < r1;
        r += (int64_t)gridDim.x * blockDim.x) {
     Acc t = ys[r];
     for (int b = 1; b < nblk; b++)
@@ -168,11 +190,43 @@ int split_blocks(const Csr &A) {
   return (int)std::min<int64_t>(kMaxBlocks, (xbytes + kSplitBlock - 1) / kSplitBlock);
 }
 
+// First column of each of nblk blocks, plus n: equal widths, or with
+// DRB_COLSPLIT_FIRST=<f> (0 < f < 1) a first block of f*n columns and equal
+// widths after it.  Empty blocks are dropped.
+std::vector<int64_t> block_bounds(int64_t n, int nblk) {
+  double first = 0.0;
+  if (const char *e = std::getenv("DRB_COLSPLIT_FIRST"))
+    first = std::atof(e);
+  std::vector<int64_t> c(1, 0);
+  if (first > 0.0 && first < 1.0) {
+    const int64_t c1 = std::min(n - 1, std::max<int64_t>(1, (int64_t)(first * (double)n)));
+    c.push_back(c1);
+    const int64_t w = (n - c1 + nblk - 2) / (nblk - 1);
+    for (int b = 2; b < nblk; b++)
+      c.push_back(std::min(n, c1 + (b - 1) * w));
+  } else {
+    const int64_t w = (n + nblk - 1) / nblk;
+    for (int b = 1; b < nblk; b++)
+      c.push_back(std::min(n, b * w));
+  }
+  c.push_back(n);
+  c.erase(std::unique(c.begin(), c.end()), c.end()); // drop empty blocks
+  return c;
+}
+
+Bounds device_bounds(const std::vector<int64_t> &c) {
+  Bounds B{};
+  B.nblk = (int)c.size() - 1;
+  for (int b = 0; b < B.nblk; b++)
+    B.c[b] = c[b];
+  return B;
+}
+
 template <class V, class CI, class RI>
 drb_status scatter_typed(Csr &A, cudaStream_t s) {
   const Csr &S = *A.csplit;
   split_scatter<CI, RI, V><<<warp_grid(A.m), 256, 0, s>>>(
-      A.rowptr.as<RI>(), A.colind.as<CI>(), A.vals.as<V>(), A.m, A.cbw, A.csplit_nblk,
+      A.rowptr.as<RI>(), A.colind.as<CI>(), A.vals.as<V>(), A.m, device_bounds(A.cbounds),
       S.rowptr.as<RI>(), S.colind.as<CI>(), S.vals.as<V>());
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
@@ -182,8 +236,8 @@ drb_status scatter_typed(Csr &A, cudaStream_t s) {
 template <class V, class CI, class RI>
 drb_status build_typed(Csr &A, int nblk, int tile, cudaStream_t s) {
   const int64_t m = A.m;
-  const int64_t bw = (A.n + nblk - 1) / nblk;
-  nblk = (int)((A.n + bw - 1) / bw); // every block holds at least one column
+  const std::vector<int64_t> bounds = block_bounds(A.n, nblk);
+  nblk = (int)bounds.size() - 1; // every block holds at least one column
   if (nblk < 2)
     return DRB_OK;
   const int64_t mv = (int64_t)nblk * (m + 1) - 1; // rows of the virtual matrix
@@ -217,7 +271,7 @@ drb_status build_typed(Csr &A, int nblk, int tile, cudaStream_t s) {
     DRB_TRY(cnt.alloc(sizeof(RI) * (mv + 1)));
     DRB_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, cnt.bytes, s));
     split_count<CI, RI><<<warp_grid(m), 256, 0, s>>>(A.rowptr.as<RI>(), A.colind.as<CI>(),
-                                                     m, bw, nblk, cnt.as<RI>());
+                                                     m, device_bounds(bounds), cnt.as<RI>());
     note_launch();
     DRB_CUDA_TRY(cudaGetLastError());
     size_t tmp_bytes = 0;
@@ -255,7 +309,7 @@ drb_status build_typed(Csr &A, int nblk, int tile, cudaStream_t s) {
   DRB_TRY(A.csplit_y.alloc((size_t)(mv + 1) * ab));
   A.csplit = std::move(S);
   A.csplit_nblk = nblk;
-  A.cbw = bw;
+  A.cbounds = bounds;
   DRB_TRY(scatter_typed<V, CI, RI>(A, s));
   std::vector<RI> rp_h(mv + 1);
   DRB_CUDA_TRY(cudaMemcpyAsync(rp_h.data(), A.csplit->rowptr.p, sizeof(RI) * (mv + 1),
@@ -293,7 +347,7 @@ drb_status colsplit_build(Csr &A, cudaStream_t s) {
   A.csplit.reset();
   A.csplit_y.release();
   A.csplit_nblk = 0;
-  A.cbw = 0;
+  A.cbounds.clear();
   const int nblk = split_blocks(A);
   if (nblk < 2)
     return DRB_OK;
@@ -308,18 +362,217 @@ drb_status colsplit_refresh_values(Csr &A, cudaStream_t s) {
   return A.storage == DRB_F64 ? scatter_v<double>(A, s) : scatter_v<float>(A, s);
 }
 
-drb_status colsplit_launch(Csr &A, const void *x, void *y, cudaStream_t s) {
-  DRB_TRY(spmv_pipe_launch(*A.csplit, x, A.csplit_y.p, s));
+namespace {
+// y[r0, r1) from the blocks' partial sums.
+drb_status combine_rows(Csr &A, void *y, int64_t r0, int64_t r1, cudaStream_t s) {
+  if (r1 <= r0)
+    return DRB_OK;
+  const unsigned g = flat_grid(r1 - r0);
   if (A.storage == DRB_F64)
-    split_combine<double><<<flat_grid(A.m), 256, 0, s>>>(A.csplit_y.as<double>(),
-                                                         static_cast<double *>(y), A.m,
-                                                         A.csplit_nblk);
+    split_combine<double><<<g, 256, 0, s>>>(A.csplit_y.as<double>(), static_cast<double *>(y),
+                                            A.m, r0, r1, A.csplit_nblk);
   else
-    split_combine<float><<<flat_grid(A.m), 256, 0, s>>>(A.csplit_y.as<float>(),
-                                                        static_cast<float *>(y), A.m,
-                                                        A.csplit_nblk);
+    split_combine<float><<<g, 256, 0, s>>>(A.csplit_y.as<float>(), static_cast<float *>(y),
+                                           A.m, r0, r1, A.csplit_nblk);
   note_launch();
   DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
+}
+} // namespace
+
+drb_status colsplit_launch(Csr &A, const void *x, void *y, cudaStream_t s) {
+  DRB_TRY(spmv_pipe_launch(*A.csplit, x, A.csplit_y.p, s));
+  return combine_rows(A, y, 0, A.m, s);
+}
+
+namespace {
+
+constexpr int kSplitHostSegments = 6; // row segments of the last block
+// Each of the last block's segments holds this multiple of the previous one's
+// nonzeros: the last block computes about as fast as its rows copy back over
+// PCIe, so a smaller first segment starts the copy earlier while the later,
+// larger ones still finish before the copy reaches them.  Measured on a
+// 16.8M-row power-law matrix (FP32 in two blocks, FP64 in three; ms per call,
+// pinned buffers): 2 to 6 segments at growth 0.8 / 1.0 / 1.25: FP32 3.16 /
+// 3.09 / 3.06 (2) ... 2.93 / 2.86 / 2.84 (6), FP64 5.77 / 5.73 / 5.69 (2) ...
+// 5.54 / 5.45 / 5.37 (6); growth 1.5 and 2.0 lost on FP32 (+1-2 %, +8 %).
+constexpr double kSplitSegmentGrowth = 1.25;
+
+int split_host_segments() {
+  const char *e = std::getenv("DRB_HOST_SEGMENTS");
+  if (!e || !*e)
+    return kSplitHostSegments;
+  return std::min(64, std::max(1, std::atoi(e)));
+}
+
+// DRB_HOST_SPLIT_GROWTH (0.2..5) overrides the growth, read with the count.
+double split_segment_growth() {
+  const char *e = std::getenv("DRB_HOST_SPLIT_GROWTH");
+  if (!e || !*e)
+    return kSplitSegmentGrowth;
+  return std::min(5.0, std::max(0.2, std::atof(e)));
+}
+
+// Orders the virtual matrix's items by row and cuts them for the host-pointer
+// gemv.  An item belongs to the block of its last row (an item may run from
+// one block's last rows over the empty separator into the next block's first
+// rows; the x slices arrive in order, so it waits for the later one).  Every
+// block but the last is one segment; the last is cut into `target` row
+// segments whose nonzeros grow by `growth`, each cut before a whole-row item
+// or a row's first chunk, so a split row never straddles two segments.
+drb_status build_host_segments(Csr &A, int target, double growth) {
+  Csr &S = *A.csplit;
+  PipePlan &P = S.pipe;
+  const int nb = A.csplit_nblk;
+  const int64_t stride = A.m + 1;
+  std::vector<Item> it((size_t)P.nitems);
+  DRB_CUDA_TRY(cudaMemcpy(it.data(), P.items.p, sizeof(Item) * it.size(),
+                          cudaMemcpyDeviceToHost));
+  std::stable_sort(it.begin(), it.end(),
+                   [](const Item &a, const Item &b) { return a.r0 < b.r0; });
+  auto blk = [&](const Item &t) {
+    const int64_t last = (int64_t)t.r0 + std::max<int64_t>(t.nrows, 1) - 1;
+    return (int)std::min<int64_t>(nb - 1, last / stride);
+  };
+  // the last block's first item and its nonzeros
+  size_t lb = 0;
+  while (lb < it.size() && blk(it[lb]) < nb - 1)
+    lb++;
+  int64_t total = 0;
+  for (size_t i = lb; i < it.size(); i++)
+    total += it[i].len;
+  std::vector<double> cut; // running nnz (within the last block) of each later segment's start
+  {
+    double w = 1.0, wsum = 0.0;
+    for (int j = 0; j < target; j++, w *= growth)
+      wsum += w;
+    w = 1.0;
+    for (double acc = 0.0; (int)cut.size() < target - 1; w *= growth) {
+      acc += w;
+      cut.push_back((double)total * acc / wsum);
+    }
+  }
+  P.seg_i0.assign(1, 0);
+  P.seg_r0.assign(1, 0);
+  P.seg_blk.assign(1, it.empty() ? nb - 1 : blk(it[0]));
+  int64_t acc = 0;
+  size_t j = 0;
+  for (size_t i = 1; i < it.size(); i++) {
+    const int b = blk(it[i]);
+    if (i > lb)
+      acc += it[i - 1].len;
+    const bool new_row = it[i].nrows > 0 || it[i].r0 != it[i - 1].r0;
+    bool cut_here = b != blk(it[i - 1]); // a new block (never inside a split row)
+    if (!cut_here && b == nb - 1 && i > lb && j < cut.size() && (double)acc >= cut[j] &&
+        new_row) {
+      cut_here = true;
+      j++;
+    }
+    if (cut_here) {
+      P.seg_i0.push_back((int64_t)i);
+      P.seg_r0.push_back(it[i].r0);
+      P.seg_blk.push_back(b);
+    }
+  }
+  P.seg_i0.push_back((int64_t)it.size());
+  P.seg_r0.push_back(S.m + 1);
+  // chunks are numbered in row order and a split row stays in one segment,
+  // so segment g's chunks are the contiguous range [seg_c0[g], seg_c0[g+1])
+  P.seg_c0.assign(1, 0);
+  for (size_t g = 0; g + 1 < P.seg_i0.size(); g++) {
+    int64_t cend = P.seg_c0.back();
+    for (int64_t i = P.seg_i0[g]; i < P.seg_i0[g + 1]; i++)
+      if (it[(size_t)i].nrows == 0)
+        cend = std::max<int64_t>(cend, (int64_t)it[(size_t)i].chunk + 1);
+    P.seg_c0.push_back(cend);
+  }
+  DRB_TRY(P.seg_items.alloc(sizeof(Item) * std::max<size_t>(it.size(), 1)));
+  if (!it.empty())
+    DRB_CUDA_TRY(cudaMemcpy(P.seg_items.p, it.data(), sizeof(Item) * it.size(),
+                            cudaMemcpyHostToDevice));
+  return DRB_OK;
+}
+
+} // namespace
+
+drb_status colsplit_gemv_host(Csr &A, const void *x_host, void *y_host, size_t xb,
+                              size_t yb, cudaStream_t s) {
+  Csr &S = *A.csplit;
+  PipePlan &P = S.pipe;
+  const int nb = A.csplit_nblk;
+  if (P.seg_i0.empty() || P.seg_blk.size() + 1 != P.seg_i0.size())
+    DRB_TRY(build_host_segments(A, split_host_segments(), split_segment_growth()));
+  const int nseg = (int)P.seg_i0.size() - 1;
+  const int64_t base = (int64_t)(nb - 1) * (A.m + 1); // first virtual row of the last block
+  if (!A.copy_stream)
+    DRB_CUDA_TRY(cudaStreamCreateWithFlags(&A.copy_stream, cudaStreamNonBlocking));
+  // events: [start][x block 0 .. nb-1][segment 0 .. nseg-1][end]
+  while ((int)A.seg_done.size() < nseg + nb + 2) {
+    cudaEvent_t e;
+    DRB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    A.seg_done.push_back(e);
+  }
+  cudaEvent_t *ev = A.seg_done.data();
+  // the copies follow the work already queued on s
+  DRB_CUDA_TRY(cudaEventRecord(ev[0], s));
+  DRB_CUDA_TRY(cudaStreamWaitEvent(A.copy_stream, ev[0], 0));
+  for (int b = 0; b < nb; b++) {
+    const int64_t c0 = A.cbounds[b], c1 = A.cbounds[b + 1];
+    DRB_CUDA_TRY(cudaMemcpyAsync(A.xh_dev.as<char>() + xb * c0,
+                                 static_cast<const char *>(x_host) + xb * c0, xb * (c1 - c0),
+                                 cudaMemcpyHostToDevice, A.copy_stream));
+    DRB_CUDA_TRY(cudaEventRecord(ev[1 + b], A.copy_stream));
+  }
+  // real rows of segment g (the last block's segments; empty for the others)
+  auto rows = [&](int g, int64_t &r0, int64_t &r1) {
+    r0 = std::min(A.m, std::max<int64_t>(0, P.seg_r0[g] - base));
+    r1 = g + 1 == nseg ? A.m : std::min(A.m, std::max<int64_t>(0, P.seg_r0[g + 1] - base));
+    if (P.seg_blk[g] != nb - 1)
+      r0 = r1 = 0;
+  };
+  // the kernel reads P.items / P.nitems: point them at one segment at a time;
+  // all launches first (a copy into pageable host memory would block this
+  // thread), then the copies back, each behind its segment's event
+  void *items0 = P.items.p;
+  const int64_t n0 = P.nitems;
+  drb_status st = DRB_OK;
+  int waited = -1;
+  for (int g = 0; g < nseg && st == DRB_OK; g++) {
+    for (; waited < P.seg_blk[g] && st == DRB_OK; waited++)
+      if (cudaStreamWaitEvent(s, ev[2 + waited], 0) != cudaSuccess)
+        st = DRB_ERR_CUDA;
+    if (st != DRB_OK)
+      break;
+    P.items.p = P.seg_items.as<Item>() + P.seg_i0[g];
+    P.nitems = P.seg_i0[g + 1] - P.seg_i0[g];
+    P.fin_c0 = P.seg_c0[g];
+    P.fin_c1 = P.seg_c0[g + 1];
+    st = spmv_pipe_launch(S, A.xh_dev.p, A.csplit_y.p, s);
+    P.items.p = items0;
+    P.nitems = n0;
+    P.fin_c0 = 0;
+    P.fin_c1 = -1;
+    int64_t r0, r1;
+    rows(g, r0, r1);
+    if (st == DRB_OK)
+      st = combine_rows(A, A.yh_dev.p, r0, r1, s);
+    if (st == DRB_OK && cudaEventRecord(ev[1 + nb + g], s) != cudaSuccess)
+      st = DRB_ERR_CUDA;
+  }
+  DRB_TRY(st);
+  for (int g = 0; g < nseg; g++) {
+    int64_t r0, r1;
+    rows(g, r0, r1);
+    if (r1 <= r0)
+      continue;
+    DRB_CUDA_TRY(cudaStreamWaitEvent(A.copy_stream, ev[1 + nb + g], 0));
+    DRB_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(y_host) + yb * r0,
+                                 A.yh_dev.as<char>() + yb * r0, yb * (r1 - r0),
+                                 cudaMemcpyDeviceToHost, A.copy_stream));
+  }
+  DRB_CUDA_TRY(cudaEventRecord(ev[nseg + nb + 1], A.copy_stream));
+  DRB_CUDA_TRY(cudaStreamWaitEvent(s, ev[nseg + nb + 1], 0));
+  DRB_CUDA_TRY(cudaStreamSynchronize(s));
   return DRB_OK;
 }
 

@@ -151,6 +151,7 @@ struct PipePlan {
   DevBuf seg_items;
   std::vector<int64_t> seg_i0, seg_r0;
   std::vector<int64_t> seg_c0;      // first chunk of each segment (+ end)
+  std::vector<int> seg_blk;         // column-split plans: the x block each segment waits for
   int64_t fin_c0 = 0, fin_c1 = -1;  // chunks the plain launch finishes (-1: all)
   uint64_t gen = 0; // bumped by every (re)build
 };
@@ -226,12 +227,12 @@ struct Csr {
   std::vector<int64_t> rowptr_h;
   // column-blocked copy for the single-RHS gemv when x does not stay in L2
   // (colsplit.cu): a virtual CSR whose row b*(m+1) + r holds row r's nonzeros
-  // of columns [b*cbw, (b+1)*cbw), its block-major partial sums and the block
-  // count (0: no split)
+  // of columns [cbounds[b], cbounds[b+1]), its block-major partial sums and the
+  // block count (0: no split)
   std::unique_ptr<Csr> csplit;
   DevBuf csplit_y;
   int csplit_nblk = 0;
-  int64_t cbw = 0;
+  std::vector<int64_t> cbounds;
   ~Csr();
 };
 
@@ -279,6 +280,12 @@ drb_status colsplit_build(Csr &A, cudaStream_t s);
 drb_status colsplit_refresh_values(Csr &A, cudaStream_t s);
 drb_status colsplit_launch(Csr &A, const void *x, void *y, cudaStream_t s);
 drb_status colsplit_tune(Csr &A, cudaStream_t s);
+// The host-pointer gemv of a column-split handle: x goes up block by block and
+// each block's items run as soon as its slice has arrived; the last block runs
+// in row segments whose rows copy back while later ones compute.  y is
+// bit-identical to colsplit_launch's.
+drb_status colsplit_gemv_host(Csr &A, const void *x_host, void *y_host, size_t xb,
+                              size_t yb, cudaStream_t s);
 drb_status abar_launch(Csr &A, const void *ybar, const void *x, void *abar,
                        cudaStream_t s);
 drb_status residual_launch(Csr &A, const void *x, const void *b, void *y,

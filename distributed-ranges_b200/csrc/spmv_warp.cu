@@ -130,6 +130,7 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
   }
   plan.seg_items.release(); // the row-segment order is rebuilt on demand
   plan.seg_c0.clear();
+  plan.seg_blk.clear();
   plan.seg_i0.clear();
   plan.seg_r0.clear();
   plan.nitems = (int64_t)all.size();

@@ -419,8 +419,8 @@ class distributed_sparse_matrix:
         return v.value
 
     def column_blocks(self):
-        """(blocks, block width) of the single-RHS product's column split
-        (drb_csr_column_blocks): (1, n) when x stays in L2."""
+        """(blocks, first block's width) of the single-RHS product's column
+        split (drb_csr_column_blocks): (1, n) when x stays in L2."""
         nb, bw = C.c_int(), C.c_int64()
         check(capi.lib.drb_csr_column_blocks(self._h, C.byref(nb), C.byref(bw)))
         return nb.value, bw.value

@@ -156,7 +156,10 @@ drb_status drb_csr_gemv(drb_csr_t A, const void *x, void *y, int64_t k,
 
 /* Same product with HOST x and y (any host memory; pinned is fastest): the
  * call copies x to the device, multiplies, copies y back and synchronises,
- * as gemv(root, res, A, x) returns res on the host. */
+ * as gemv(root, res, A, x) returns res on the host.  For k = 1 the copies
+ * overlap the product (y comes back in row segments behind the compute, and
+ * a column-split handle also uploads x block by block ahead of it); y has
+ * the bits of drb_csr_gemv. */
 drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
                              int64_t k, drb_layout layout, void *stream);
 
@@ -179,21 +182,25 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
 /* Column blocks of the single right-hand-side product (no counterpart in the
  * reference; a layout choice inside the handle).  A randomly gathered x stays
  * in B200's L2 only up to about 48 MB, so drb_csr_create regroups the
- * nonzeros of an F32/F64 handle whose x is larger than 64 MiB (and that
- * reuses x at least twice, nnz >= 2n) into *nblocks column blocks of
- * *block_width columns (x slices of at most 48 MiB), kept as a second copy
- * of the values and column indices on the device (block-major: every row's
- * nonzeros of block 0, then of block 1, ...), with nblocks partial sums per
- * row of scratch, when that fits with 1 GB to spare.  gemv (k = 1, device or
- * host pointers) then runs one launch over the copy -- its warps move through
- * the blocks in order, so one x slice at a time is hot in L2 -- and a short
- * pass that adds each row's block sums in block order: deterministic, the
- * same bits from drb_csr_gemv and drb_csr_gemv_host.  The adjoint's
- * transposed matrix is split the same way.  The environment variable
- * DRB_COLSPLIT=<n> (read when a handle is created) asks for n blocks (0 or 1:
- * none).  A handle on its sliced-ELL copy (short regular rows, whose gathers
- * are local) is not split.  *nblocks = 1 (and *block_width = n) when the
- * handle is not split. */
+ * nonzeros of an F32/F64 handle whose x is larger than 48 MiB (and that
+ * reuses x at least twice, nnz >= 2n) into *nblocks column blocks (x slices
+ * of at most 48 MiB; *block_width is the first block's width, the others
+ * share the remaining columns equally), kept as a second copy of the values
+ * and column indices on the device (block-major: every row's nonzeros of
+ * block 0, then of block 1, ...), with nblocks partial sums per row of
+ * scratch, when that fits with 1 GB to spare.  drb_csr_gemv (k = 1) then runs
+ * one launch over the copy -- its warps move through the blocks in order, so
+ * one x slice at a time is hot in L2 -- and a short pass that adds each row's
+ * block sums in block order.  drb_csr_gemv_host pipelines the same work over
+ * the blocks: x goes up slice by slice, each block runs once its slice has
+ * arrived, and the last block runs in row segments whose rows copy back
+ * while the later segments compute.  Both are deterministic and give the same
+ * bits.  The adjoint's transposed matrix is split the same way.  The
+ * environment variables DRB_COLSPLIT=<n> (n blocks; 0 or 1: none) and
+ * DRB_COLSPLIT_FIRST=<f> (a first block of f*n columns), read when a handle
+ * is created, override the choice.  A handle on its sliced-ELL copy (short
+ * regular rows, whose gathers are local) is not split.  *nblocks = 1 (and
+ * *block_width = n) when the handle is not split. */
 drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width);
 
 /* Synchronise `stream` and report device-side failures of earlier launches

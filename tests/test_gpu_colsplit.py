@@ -85,6 +85,43 @@ def test_split_gemv_parity(mp, dtype, nblk, unsorted, monkeypatch):
     a.destroy()
 
 
+@pytest.mark.parametrize("nblk,first,segs,growth", [
+    (2, "0.3", "6", "1.5"), (2, "0.45", "1", "1.5"), (3, "", "8", "0.7"),
+    (2, "0.7", "3", "2.0"), (8, "0.05", "5", "1.2")])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_split_host_pipeline(mp, dtype, nblk, first, segs, growth, monkeypatch):
+    """The host-pointer gemv of a split handle uploads x block by block, runs
+    each block once its slice has arrived and the last block in row segments
+    whose rows copy back behind the later ones: the device call's bits, for an
+    uneven first block (DRB_COLSPLIT_FIRST) and any segment count and growth,
+    with pinned and pageable host buffers, call after call."""
+    monkeypatch.setenv("DRB_COLSPLIT", str(nblk))
+    monkeypatch.setenv("DRB_COLSPLIT_FIRST", first)
+    monkeypatch.setenv("DRB_HOST_SEGMENTS", segs)
+    monkeypatch.setenv("DRB_HOST_SPLIT_GROWTH", growth)
+    rp, ci, v, m, n = mixed_rows(dtype, True, seed=41)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    nb, bw = a.column_blocks()
+    assert nb == nblk
+    if first:
+        assert bw == int(float(first) * n)
+    x = np.random.default_rng(42).uniform(-1, 1, n).astype(dtype)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.empty(m, dtype=xt.dtype, device="cuda")
+    a.gemv_device(xt, yt)
+    yd = yt.cpu().numpy()
+    check(yd, rp, ci, v, x, m, n, 1e-5 if dtype == np.float32 else 1e-12)
+    xp = torch.from_numpy(x).pin_memory()
+    yp = torch.full((m,), float("nan"), dtype=xp.dtype).pin_memory()
+    for _ in range(2):
+        a.gemv_host(xp.numpy(), yp.numpy())
+        assert np.array_equal(yp.numpy().view(np.uint8), yd.view(np.uint8))
+    yh = np.full(m, np.nan, dtype)
+    a.gemv_host(x, yh)
+    assert np.array_equal(yh.view(np.uint8), yd.view(np.uint8))
+    a.destroy()
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_split_matches_unsplit_within_tolerance(mp, dtype, monkeypatch):
     """The same handle without a split (DRB_COLSPLIT=0): both within the gate
