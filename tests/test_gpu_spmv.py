@@ -597,6 +597,42 @@ def test_abar_short_rows_edges(mp, dtype, m):
     assert np.array_equal(abar.cpu().numpy(), yb[rows] * x[ci])
 
 
+@pytest.mark.parametrize("variant", ["128,1", "256,0", "512,1", "128,1,1"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_abar_items_edges(mp, dtype, variant, monkeypatch):
+    """A longest row above 64 nonzeros sends abar to the forward product's
+    work items (one item ahead, rows from stamps and a warp max-scan): empty
+    rows, runs of 0-2 nonzero rows (64-row items), rows split into chunks of
+    every item span, and an output not 16-byte aligned (scalar stores); one
+    rounded product per entry, so numpy's bits."""
+    monkeypatch.setenv("DRB_SPMV_VARIANT", variant)
+    rng = np.random.default_rng(11)
+    n = 5000
+    lens = np.concatenate([rng.integers(0, 3, 3000), [0, 0, 1, 2000, 0, 70, 129, 257, 513, 0],
+                           rng.integers(0, 200, 300), rng.integers(0, 2, 1000), [64, 65, 0]])
+    m = len(lens)
+    rp = np.zeros(m + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(n, k, replace=False)) for k in lens]).astype(np.int32)
+    v = rng.uniform(-1, 1, len(ci)).astype(dtype)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    yb = rng.uniform(-1, 1, m).astype(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0, adjoint=True)
+    assert a.variant() & ~3 == int(variant.split(",")[0])
+    tdt = torch.from_numpy(x).dtype
+    ref = yb[np.repeat(np.arange(m), lens)] * x[ci]
+    xt, ybt = torch.from_numpy(x).cuda(), torch.from_numpy(yb).cuda()
+    for shift in (0, 1):  # 1: abar one element past a 16-byte boundary
+        buf = torch.full((len(v) + 1,), 7.0, dtype=tdt, device="cuda")
+        abar = buf[shift:shift + len(v)]
+        for _ in range(2):
+            mp.gemv_backward(a, ybt, xt, None, abar)
+        a.check()
+        assert np.array_equal(abar.cpu().numpy(), ref)
+        assert buf[len(v) if shift == 0 else 0].item() == 7.0  # nothing outside abar written
+    a.destroy()
+
+
 def test_adjoint_finite_differences_laplacian(mp):
     """Central differences (h = 1e-6, fp64) of L = 0.5 ||A x - b||^2 through
     the forward gemv.  The loss difference is formed row by row as
