@@ -184,8 +184,10 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
  * in B200's L2 only up to about 48 MB, so drb_csr_create regroups the
  * nonzeros of an F32/F64 handle whose x is larger than 48 MiB (and that
  * reuses x at least twice, nnz >= 2n) into *nblocks column blocks (x slices
- * of at most 48 MiB; *block_width is the first block's width, the others
- * share the remaining columns equally), kept as a second copy of the values
+ * of at most 48 MiB; *block_width is the first block's width: 45% of the
+ * columns when there are two, so that the host-pointer call's first block
+ * finishes as x's last slice lands; the others share the remaining columns
+ * equally), kept as a second copy of the values
  * and column indices on the device (block-major: every row's nonzeros of
  * block 0, then of block 1, ...), with nblocks partial sums per row of
  * scratch, when that fits with 1 GB to spare.  drb_csr_gemv (k = 1) then runs
@@ -197,8 +199,8 @@ drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
  * while the later segments compute.  Both are deterministic and give the same
  * bits.  The adjoint's transposed matrix is split the same way.  The
  * environment variables DRB_COLSPLIT=<n> (n blocks; 0 or 1: none) and
- * DRB_COLSPLIT_FIRST=<f> (a first block of f*n columns), read when a handle
- * is created, override the choice.  A handle on its sliced-ELL copy (short
+ * DRB_COLSPLIT_FIRST=<f> (a first block of f*n columns, 0 < f < 1; any other
+ * value: equal widths), read when a handle is created, override the choice.  A handle on its sliced-ELL copy (short
  * regular rows, whose gathers are local) is not split.  *nblocks = 1 (and
  * *block_width = n) when the handle is not split. */
 drb_status drb_csr_column_blocks(drb_csr_t A, int *nblocks, int64_t *block_width);
