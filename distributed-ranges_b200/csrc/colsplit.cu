@@ -149,16 +149,110 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Row sums over the blocks of four grid-stride rows at once (their loads
+// first, so each thread keeps 4 * nblk loads in flight): t[u] = sum over
+// blocks b (in order) of ys[b * (m + 1) + row u]; rows at or past r1 give 0.
+constexpr int kCombineRows = 4;
+
+template <class Acc>
+__device__ __forceinline__ void combine4(const Acc *__restrict__ ys, int64_t m, int64_t r,
+                                         int64_t stride, int64_t r1, int nblk,
+                                         Acc (&t)[kCombineRows]) {
+#pragma unroll
+  for (int u = 0; u < kCombineRows; u++)
+    t[u] = r + u * stride < r1 ? ys[r + u * stride] : Acc(0);
+  for (int b = 1; b < nblk; b++) {
+    Acc a[kCombineRows];
+#pragma unroll
+    for (int u = 0; u < kCombineRows; u++)
+      a[u] = r + u * stride < r1 ? ys[(int64_t)b * (m + 1) + r + u * stride] : Acc(0);
+#pragma unroll
+    for (int u = 0; u < kCombineRows; u++)
+      t[u] += a[u];
+  }
+}
+
 // y[r] = sum over blocks b (in order) of ys[b * (m + 1) + r], rows [r0, r1).
 template <class Acc>
 __global__ void split_combine(const Acc *__restrict__ ys, Acc *__restrict__ y, int64_t m,
                               int64_t r0, int64_t r1, int nblk) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < r1;
-       r += (int64_t)gridDim.x * blockDim.x) {
-    Acc t = ys[r];
-    for (int b = 1; b < nblk; b++)
-      t += ys[(int64_t)b * (m + 1) + r];
-    y[r] = t;
+       r += kCombineRows * stride) {
+    Acc t[kCombineRows];
+    combine4(ys, m, r, stride, r1, nblk, t);
+#pragma unroll
+    for (int u = 0; u < kCombineRows; u++)
+      if (r + u * stride < r1)
+        y[r + u * stride] = t[u];
+  }
+}
+
+// split_combine with the residual ||y - b||^2 folded in: each thread adds the
+// terms (y_r - b_r)^2 of its grid-stride rows in row order (in double), a CTA's
+// threads in a fixed tree into slots[blockIdx.x], and the last CTA (ticket)
+// adds the slots in index order into *out and resets the ticket.  The grid is
+// a function of m, so the grouping is fixed and the result repeats bit for
+// bit.
+template <class Acc>
+__global__ void __launch_bounds__(256)
+    split_combine_resid(const Acc *__restrict__ ys, Acc *__restrict__ y,
+                        const Acc *__restrict__ b, int64_t m, int nblk, double *slots,
+                        int *ticket, double *out) {
+  __shared__ double s_red[8];
+  __shared__ int s_last;
+  double sum = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < m;
+       r += kCombineRows * stride) {
+    Acc t[kCombineRows], bb[kCombineRows];
+#pragma unroll
+    for (int u = 0; u < kCombineRows; u++)
+      bb[u] = r + u * stride < m ? b[r + u * stride] : Acc(0);
+    combine4(ys, m, r, stride, m, nblk, t);
+#pragma unroll
+    for (int u = 0; u < kCombineRows; u++)
+      if (r + u * stride < m) {
+        y[r + u * stride] = t[u];
+        const double d = (double)t[u] - (double)bb[u];
+        sum += d * d;
+      }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (lane == 0)
+    s_red[warp] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+      c += s_red[w];
+    slots[blockIdx.x] = c;
+    __threadfence();
+    s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last)
+    return;
+  __threadfence();
+  double t = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+    t += __ldcg(&slots[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    t += __shfl_xor_sync(0xffffffffu, t, o);
+  __syncthreads(); // s_red is reused
+  if (lane == 0)
+    s_red[warp] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double c = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+      c += s_red[w];
+    *out = c;
+    *ticket = 0;
   }
 }
 
@@ -394,6 +488,31 @@ drb_status combine_rows(Csr &A, void *y, int64_t r0, int64_t r1, cudaStream_t s)
 drb_status colsplit_launch(Csr &A, const void *x, void *y, cudaStream_t s) {
   DRB_TRY(spmv_pipe_launch(*A.csplit, x, A.csplit_y.p, s));
   return combine_rows(A, y, 0, A.m, s);
+}
+
+drb_status colsplit_residual(Csr &A, const void *x, const void *b, void *y, double *out,
+                             cudaStream_t s) {
+  DRB_TRY(spmv_pipe_launch(*A.csplit, x, A.csplit_y.p, s));
+  // per-CTA slots and the ticket: the fused-reduction scratch of A's own plan
+  // (sms * 32 doubles, then the ticket), used by one launch at a time
+  DRB_TRY(fused_scratch(A));
+  int sms = 0;
+  DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, A.device));
+  const unsigned g = std::min<unsigned>(flat_grid(A.m), (unsigned)sms * 32);
+  double *slots = A.pipe.red.as<double>();
+  int *ticket = reinterpret_cast<int *>(slots + (size_t)sms * 32);
+  if (A.storage == DRB_F64)
+    split_combine_resid<double><<<g, 256, 0, s>>>(A.csplit_y.as<double>(),
+                                                  static_cast<double *>(y),
+                                                  static_cast<const double *>(b), A.m,
+                                                  A.csplit_nblk, slots, ticket, out);
+  else
+    split_combine_resid<float><<<g, 256, 0, s>>>(A.csplit_y.as<float>(), static_cast<float *>(y),
+                                                 static_cast<const float *>(b), A.m,
+                                                 A.csplit_nblk, slots, ticket, out);
+  note_launch();
+  DRB_CUDA_TRY(cudaGetLastError());
+  return DRB_OK;
 }
 
 namespace {

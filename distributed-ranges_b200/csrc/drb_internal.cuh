@@ -279,6 +279,10 @@ drb_status autotune_pipe(Csr &A, cudaStream_t s, int *chosen);
 drb_status colsplit_build(Csr &A, cudaStream_t s);
 drb_status colsplit_refresh_values(Csr &A, cudaStream_t s);
 drb_status colsplit_launch(Csr &A, const void *x, void *y, cudaStream_t s);
+// ||A x - b||^2 on the split copy: the same launch, the residual folded into
+// the combine pass (a fixed grouping: repeatable bit for bit).
+drb_status colsplit_residual(Csr &A, const void *x, const void *b, void *y, double *out,
+                             cudaStream_t s);
 drb_status colsplit_tune(Csr &A, cudaStream_t s);
 // The host-pointer gemv of a column-split handle: x goes up block by block and
 // each block's items run as soon as its slice has arrived; the last block runs

@@ -317,6 +317,8 @@ drb_status residual_launch(Csr &A, const void *x, const void *b, void *y,
     DRB_TRY(A.ys.ensure((size_t)dtype_bytes(A.storage) * A.m));
     y = A.ys.p;
   }
+  if (A.csplit && !A.sell.on && A.m > 0)
+    return colsplit_residual(A, x, b, y, out, s);
   return residual_pipe_launch(A, x, b, y, out, s);
 }
 

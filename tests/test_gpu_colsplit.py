@@ -144,6 +144,34 @@ def test_split_matches_unsplit_within_tolerance(mp, dtype, monkeypatch):
         a.destroy()
 
 
+@pytest.mark.parametrize("nblk", [2, 3])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_split_residual(mp, dtype, nblk, monkeypatch):
+    """||A x - b||^2 on a split handle: the split launch with the residual
+    folded into the combine pass.  y has the gemv's bits (the same combine),
+    the norm is the double sum of its terms (within summation order), the
+    same bits call after call, and without a y buffer; y against the oracle."""
+    monkeypatch.setenv("DRB_COLSPLIT", str(nblk))
+    rp, ci, v, m, n = mixed_rows(dtype, False, seed=51)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    assert a.column_blocks()[0] == nblk
+    rng = np.random.default_rng(52)
+    x = rng.uniform(-1, 1, n).astype(dtype)
+    b = rng.uniform(-1, 1, m).astype(dtype)
+    xt, bt = torch.from_numpy(x).cuda(), torch.from_numpy(b).cuda()
+    y = torch.full((m,), float("nan"), dtype=xt.dtype, device="cuda")
+    outs = [mp.residual_norm2(a, xt, bt, y).item() for _ in range(3)]
+    outs.append(mp.residual_norm2(a, xt, bt).item())
+    assert len(set(outs)) == 1
+    yg = torch.empty_like(y)
+    a.gemv_device(xt, yg)
+    assert torch.equal(y, yg)
+    ref = float(((y.double() - bt.double()) ** 2).sum())
+    assert abs(outs[0] - ref) <= 1e-10 * ref
+    check(y.cpu().numpy(), rp, ci, v, x, m, n, 1e-5 if dtype == np.float32 else 1e-12)
+    a.destroy()
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_split_adjoint(mp, dtype, monkeypatch):
     """x-bar = A^T y-bar on the split transposed matrix, against the oracle's
