@@ -19,9 +19,10 @@
 // Storage and accumulation types: V is the stored element type of values and
 // x (float, double, or bfloat16 bits in uint16_t); products and sums use
 // Acc = float for float/bf16 and double for double; y has type Acc.  With
-// COMP the sums are two-sum compensated (a running sum plus the rounding
-// error of every addition, combined at the end), so a bf16 x bf16 product,
-// exact in fp32, reaches y with only the final rounding.
+// COMP the sums are two-sum compensated: a running sum plus the rounding
+// error of every addition of a block of four products (their plain sum),
+// combined at the end, so y carries the products' roundings (none for bf16 x
+// bf16), at most 3u of each block's magnitudes and the final rounding.
 //
 // On B200 the random x gathers are bounded by the SM's L1-to-crossbar request
 // rate (about one request per SM per clock); the design keeps many gathers in
@@ -237,6 +238,56 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     return t.value();
   }
 
+  // Sum of the products of a chunk item held by this lane (registers).  With
+  // COMP the products are added in blocks of four -- a plain sum, then one
+  // two-sum into the running compensated sum: a block's roundings stay below
+  // 3u of its magnitudes (u = 2^-24), far under the input rounding of a bf16
+  // operand (2^-8) and the 1e-6 accumulation gate, at a quarter of the
+  // two-sums (one per product cost ~9 % on a bf16 single-RHS product).
+  __device__ __forceinline__ void chunk_sum(const S &sl, const Acc (&xg)[NG][G], int off,
+                                            int end, int ng, CSum<Acc> &acc) const {
+    static_assert((NG * G) % 4 == 0, "blocks of four products");
+    Acc blk = Acc(0);
+#pragma unroll
+    for (int j = 0; j < NG; j++) {
+      const int g = lane + 32 * j;
+#pragma unroll
+      for (int i = 0; i < G; i++) {
+        const int q = g * G + i;
+        const bool in = g < ng && q >= off && q < end;
+        if (COMP) {
+          const Acc p = in ? to_acc(sl.v[j][i]) * xg[j][i] : Acc(0);
+          blk = add_rn(blk, p);
+          if ((j * G + i) % 4 == 3) {
+            acc.add(blk);
+            blk = Acc(0);
+          }
+        } else if (in) {
+          acc.s += to_acc(sl.v[j][i]) * xg[j][i];
+        }
+      }
+    }
+  }
+
+  // Sum of positions b + gl, b + gl + tpr, ... < e of the staged products
+  // (one lane's share of a row); with COMP in blocks of four as chunk_sum.
+  __device__ __forceinline__ void row_sum(const Acc *prod, int b, int e, int gl, int tpr,
+                                          CSum<Acc> &acc) const {
+    auto at = [&](int q) { return prod[SKEW ? skew(q) : q]; };
+    int q = b + gl;
+    if (COMP) {
+      for (; q + 3 * tpr < e; q += 4 * tpr)
+        acc.add(add_rn(add_rn(add_rn(at(q), at(q + tpr)), at(q + 2 * tpr)), at(q + 3 * tpr)));
+      Acc rest = Acc(0);
+      for (; q < e; q += tpr)
+        rest = add_rn(rest, at(q));
+      acc.add(rest);
+    } else {
+      for (; q < e; q += tpr)
+        acc.s += at(q);
+    }
+  }
+
   // Runs the item in `sl` and refills the slot with item `refill`.
   template <bool RESID>
   __device__ __forceinline__ void process(S &sl, int64_t refill, Acc *prod, int *srp,
@@ -257,21 +308,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     if (cur.nrows == 0) {
       // one chunk of a long row: sum in registers, no shared memory
       CSum<Acc> acc;
-#pragma unroll
-      for (int j = 0; j < NG; j++) {
-        const int g = lane + 32 * j;
-#pragma unroll
-        for (int i = 0; i < G; i++) {
-          const int q = g * G + i;
-          if (g < ng && q >= off && q < end) {
-            const Acc p = to_acc(sl.v[j][i]) * xg[j][i];
-            if (COMP)
-              acc.add(p);
-            else
-              acc.s += p;
-          }
-        }
-      }
+      chunk_sum(sl, xg, off, end, ng, acc);
       fetch(sl, refill);
       const Acc tot = group_sum(acc.s, acc.c, 32);
       if (lane == 0)
@@ -316,16 +353,8 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     for (int base = 0; base < nrows; base += groups) {
       const int r = base + gid;
       CSum<Acc> acc;
-      if (r < nrows) {
-        const int b = srp[r], e = srp[r + 1];
-        for (int q = b + gl; q < e; q += tpr) {
-          const Acc p = prod[SKEW ? skew(q) : q];
-          if (COMP)
-            acc.add(p);
-          else
-            acc.s += p;
-        }
-      }
+      if (r < nrows)
+        row_sum(prod, srp[r], srp[r + 1], gl, tpr, acc);
       const Acc tot = group_sum(acc.s, acc.c, tpr);
       if (r < nrows && gl == 0) {
         ptx::st_hint(y + cur.r0 + r, tot, pol_y);
@@ -371,21 +400,7 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     const int ng = (end + G - 1) / G;
     if (it.nrows == 0) {
       CSum<Acc> acc;
-#pragma unroll
-      for (int j = 0; j < NG; j++) {
-        const int g = lane + 32 * j;
-#pragma unroll
-        for (int i = 0; i < G; i++) {
-          const int q = g * G + i;
-          if (g < ng && q >= off && q < end) {
-            const Acc p = to_acc(cur.v[j][i]) * xg[j][i];
-            if (COMP)
-              acc.add(p);
-            else
-              acc.s += p;
-          }
-        }
-      }
+      chunk_sum(cur, xg, off, end, ng, acc);
       gather(nxt, xg);
       fetch(cur, refill);
       const Acc tot = group_sum(acc.s, acc.c, 32);
@@ -431,16 +446,8 @@ template <class V, class XT, class CI, class RI, int TILE, bool SKEW, bool COMP>
     for (int base = 0; base < nrows; base += groups) {
       const int r = base + gid;
       CSum<Acc> acc;
-      if (r < nrows) {
-        const int b = srp[r], e = srp[r + 1];
-        for (int q = b + gl; q < e; q += tpr) {
-          const Acc p = prod[SKEW ? skew(q) : q];
-          if (COMP)
-            acc.add(p);
-          else
-            acc.s += p;
-        }
-      }
+      if (r < nrows)
+        row_sum(prod, srp[r], srp[r + 1], gl, tpr, acc);
       const Acc tot = group_sum(acc.s, acc.c, tpr);
       if (r < nrows && gl == 0) {
         ptx::st_hint(y + it.r0 + r, tot, pol_y);

@@ -142,9 +142,10 @@ drb_status drb_csr_get_entries(drb_csr_t A, int64_t offset, int64_t count,
 
 /* y = A * x for k right-hand sides, device pointers.  Element types: x and y
  * have the storage type, except BF16 storage: x bf16 (f32 with
- * DRB_FLAG_BF16_X_F32), y f32, row sums two-sum compensated in f32 (k = 1:
- * per product, a bf16 x bf16 product being exact in f32 and a bf16 x f32 one
- * rounding once; k > 1: per block of four products, as drb_batch_*).  k > 1 runs
+ * DRB_FLAG_BF16_X_F32), y f32, row sums two-sum compensated in f32 per
+ * block of four products (a bf16 x bf16 product being exact in f32 and a
+ * bf16 x f32 one rounding once; the block sums add at most 3u of their
+ * magnitudes, as drb_batch_*).  k > 1 runs
  * the batched SpMM kernel on a batch of this one handle, built on the first
  * call with a given (k, layout) -- that call synchronises `stream`, and the
  * handle then keeps a row-major copy of X (n * k elements, rows padded to 16
