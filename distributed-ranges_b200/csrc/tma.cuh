@@ -3,7 +3,8 @@
 // Every wait is bounded: mbar_wait() gives up after kWaitNs nanoseconds of
 // %globaltimer and returns false; kernels then record DRB_ERR_TIMEOUT in a
 // device error word and leave their loops instead of hanging the GPU.
-// No copy here uses .multicast::cluster.
+// Every copy here lands in the issuing CTA's own shared memory only (no
+// cluster-wide delivery).
 #pragma once
 
 #include <cstdint>
