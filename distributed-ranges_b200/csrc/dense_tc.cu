@@ -21,7 +21,7 @@
 //               Y coalesced (column-major: 32 consecutive rows per store).
 // A loads are streamed once (HBM-bound: 32 RHS make 32 FLOP per A byte, far
 // below the tensor-core roofline), so the design goal is a full TMA ring per
-// SM.  No load uses cluster multicast.
+// SM.  Every load fills the issuing CTA's own shared memory only.
 //
 // Every mbarrier wait gives up after one second of %globaltimer (a plan can
 // shorten the limit): the CTA then records DRB_ERR_TIMEOUT in the launch's
