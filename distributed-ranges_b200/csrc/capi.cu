@@ -753,8 +753,9 @@ drb_status drb_csr_gemv_backward(drb_csr_t A, const void *ybar, const void *x,
 drb_status drb_csr_variant(drb_csr_t A, int *variant) {
   if (!A || !variant)
     return invalid("NULL argument");
-  *variant = A->sell.on ? kVariantSell
-                        : A->pipe.tile | (A->pipe.skew ? 1 : 0) | (A->pipe.two_slot ? 2 : 0);
+  // a column-split handle's gemv runs the plan of its block-major copy
+  const PipePlan &P = (A->csplit && !A->sell.on) ? A->csplit->pipe : A->pipe;
+  *variant = A->sell.on ? kVariantSell : P.tile | (P.skew ? 1 : 0) | (P.two_slot ? 2 : 0);
   return DRB_OK;
 }
 

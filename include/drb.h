@@ -176,7 +176,9 @@ drb_status drb_csr_gemv_host(drb_csr_t A, const void *x_host, void *y_host,
  * and, when the matrix qualifies, the sliced copy on this matrix's sparsity
  * pattern, keeps the fastest (also for the adjoint's transposed matrix) and
  * returns it; it synchronises `stream`.  Results are identical across
- * variants up to the summation order inside a row. */
+ * variants up to the summation order inside a row.  For a column-split handle
+ * (drb_csr_column_blocks) the variant is that of the block-major copy's plan,
+ * which gemv runs (autotuned on its own). */
 drb_status drb_csr_variant(drb_csr_t A, int *variant);
 drb_status drb_csr_autotune(drb_csr_t A, int *variant, void *stream);
 

@@ -144,6 +144,28 @@ def test_split_matches_unsplit_within_tolerance(mp, dtype, monkeypatch):
         a.destroy()
 
 
+@pytest.mark.parametrize("nblk", [2, 3, 8])
+def test_split_compensated_fp32(mp, nblk, monkeypatch):
+    """A compensated FP32 handle keeps compensated sums within each column
+    block; the combine adds the nblk block sums plainly, at most (nblk - 1)
+    roundings of sum |a x| more: within the 1e-6 gate of the compensated
+    product, and the host path gives the same bits."""
+    monkeypatch.setenv("DRB_COLSPLIT", str(nblk))
+    rp, ci, v, m, n = mixed_rows(np.float32, True, seed=61)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0,
+                                     compensated=True)
+    assert a.column_blocks()[0] == nblk
+    x = np.random.default_rng(62).uniform(-1, 1, n).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    y = torch.empty(m, device="cuda")
+    a.gemv_device(xt, y)
+    check(y.cpu().numpy(), rp, ci, v, x, m, n, 1e-6)
+    yh = np.empty(m, np.float32)
+    a.gemv_host(x, yh)
+    assert np.array_equal(yh, y.cpu().numpy())
+    a.destroy()
+
+
 @pytest.mark.parametrize("nblk", [2, 3])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_split_residual(mp, dtype, nblk, monkeypatch):
