@@ -1225,6 +1225,8 @@ def profile_case(name):
                distribution with 16,777,216 columns (x 128 MB): three column
                blocks in one launch, then split_combine;
       spmm_k16_4m  k = 16 column-major on the powerlaw4m matrix (X 1.07 GB);
+      abar4m   the adjoint's abar = ybar_i x_j on the powerlaw4m matrix (FP32,
+               the forward product's work items, DRB_SPMV_VARIANT's span);
       batch16_bf16  the batched SpMM of batch16 with BF16 storage and X
                (compensated sums)."""
     import torch
@@ -1297,6 +1299,18 @@ def profile_case(name):
         mp.conjugate_gradient(A, b, x, max_iters=8, rtol=0.0)
         x.zero_()
         mp.conjugate_gradient(A, b, x, max_iters=24, rtol=0.0)
+    elif name == "abar4m":
+        alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
+        rp, ci, v = drb.gen.powerlaw_csr(4_194_304, N_COLS, alpha=alpha, hi=ZIPF_HI,
+                                         seed=SEED)
+        A = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (4_194_304, N_COLS)),
+                                         0, distr=mp.csr_row_distribution, adjoint=True)
+        x = torch.from_numpy(drb.gen.values(N_COLS, seed=SEED + 1)).cuda()
+        yb = torch.from_numpy(drb.gen.values(4_194_304, seed=SEED + 2)).cuda()
+        abar = torch.empty(len(v), device="cuda")
+        for _ in range(4):
+            mp.gemv_backward(A, yb, x, None, abar)
+        A.check()
     elif name in ("probe4m", "colsplit_f64_4m", "spmm_k16_4m"):
         alpha = drb.gen.zipf_alpha_for_mean(1, ZIPF_HI, ZIPF_MEAN)
         rp, ci, v = drb.gen.powerlaw_csr(4_194_304, N_COLS, alpha=alpha, hi=ZIPF_HI,
@@ -1387,7 +1401,8 @@ def main():
     ap.add_argument("--profile-case", choices=["batch16", "batch16_bf16", "dense64", "dense_f32",
                                                "laplacian_f64", "cg_f64", "powerlaw4m",
                                                "residual4m", "dot_f32", "adjoint_lap_f32",
-                                               "probe4m", "colsplit_f64_4m", "spmm_k16_4m"],
+                                               "probe4m", "colsplit_f64_4m", "spmm_k16_4m",
+                                               "abar4m"],
                     help="run one kernel on a small case (for ncu) and exit")
     args = ap.parse_args()
     if args.profile_case:
