@@ -516,6 +516,31 @@ def extras(args, A, rp, ci, v, x, xd, yd, nnz, bytes32, fwd_ms, stream):
         record_parity("spmm_k16_colmajor", oracle.csr_check(rp, ci, v, X16.cpu().numpy(), M,
                                                             N_COLS, Y16.cpu().numpy(), k=k16),
                       1e-5)
+    # Row-major X and Y: no packing pass, the SpMM kernel alone; beside it a
+    # plain streaming row gather on the same X (column indices and values
+    # streamed in nonzero order, the 64-byte X row gathered at each, no rows
+    # or Y): the random 64-byte reads of 1.07 GB of X, not the SM, bound both
+    import drb_probe
+    from drb import _capi as capi
+    X16.copy_(X16.view(k16, N_COLS).t().reshape(-1))
+    A.gemv_device(X16, Y16, k16, capi.DRB_ROW_MAJOR)
+    rm_ms = statistics.mean(timed_launches(
+        lambda: A.gemv_device(X16, Y16, k16, capi.DRB_ROW_MAJOR), steps, stream))
+    drb_probe.gather_rows_probe(A, X16, k16)
+    probe_ms = statistics.mean(timed_launches(lambda: drb_probe.gather_rows_probe(A, X16, k16),
+                                              steps, stream))
+    out["spmm_k16"].update({
+        "row_major_ms": round(rm_ms, 4),
+        "pack_and_y_layout_ms": round(ms - rm_ms, 4),
+        "row_gather_probe_ms": round(probe_ms, 4),
+        "row_major_vs_probe": round(probe_ms / rm_ms, 4),
+        "probe_what": "drb_csr_gather_rows_probe: column indices and values streamed in "
+                      "nonzero order, the 64-byte X row gathered at every nonzero (16-byte "
+                      "read-only loads, 4 in flight per lane), no rows or Y"})
+    if checks_on(args):
+        record_parity("spmm_k16_rowmajor", oracle.csr_check(
+            rp, ci, v, X16.view(N_COLS, k16).t().contiguous().cpu().numpy().reshape(-1), M,
+            N_COLS, Y16.view(M, k16).t().contiguous().cpu().numpy().reshape(-1), k=k16), 1e-5)
     del X16, Y16
 
     # FP64 SpMV on the same pattern

@@ -584,77 +584,139 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
 }
 
 // dst[r*ldx + j] = X(r, j) for j < k, 0 for k <= j < ldx, from column-major
-// (src[r + j*n]) or row-major (src[r*k + j]) X.  A CTA moves a tile of
-// 2^LTR rows x 2^LCW columns through shared memory (row stride 2^LTR + 1,
-// conflict-free both ways): column-major sources are read one column at a
-// time (coalesced), and with vec the tile's rows are written as 16-byte
-// vectors.  blockIdx.x is a tile of the whole batch, mapped to its matrix by
-// binary search of the tile offsets.
-template <class T, bool COLMAJOR>
-__global__ void __launch_bounds__(256)
-    batch_pack(const PackEnt *__restrict__ ents, int count, int64_t k,
-               int64_t ldx, int lcw, int ltr, int ctiles, int vec) {
+// (src[r + j*n]) or row-major (src[r*k + j]) X.  The unit is a tile of 32
+// rows x 2^LCW columns, and a persistent grid's warps take tiles w, w + W,
+// ...  For a tile every lane loads its row's elements of the tile's columns
+// at once (column-major: one coalesced line per column), the warp transposes
+// them through its shared buffer (row stride 2^LCW + 1: conflict-free
+// writes) and stores the tile's rows -- for a tile of whole packed rows one
+// contiguous run -- as 16-byte vectors (scalars when a row piece is not a
+// multiple of 16 bytes).  The next tile's loads are issued before the
+// current tile is stored, so a warp always has a tile's lines in flight.
+// (A CTA moving one tile through a 2^LTR-row buffer kept one or two loads
+// per thread in flight and packed at a quarter of HBM speed.)  A tile is
+// mapped to its matrix by binary search of the tile offsets; no CTA
+// barrier, each warp is independent.
+constexpr int kPackWarps = 4;
+
+template <class T> struct PackTile {
+  const T *in;    // this lane's first source element (column cb of its row)
+  int64_t stride; // elements between a row's consecutive source columns
+  T *out;         // the tile's first packed element (row r0, column cb)
+  int nr, nc, kc; // rows, packed columns, source columns of the tile
+};
+
+template <class T, bool COLMAJOR, int CW>
+__global__ void __launch_bounds__(kPackWarps * 32)
+    batch_pack(const PackEnt *__restrict__ ents, int count, int64_t k, int64_t ldx, int lcw,
+               int ctiles, int64_t ntiles) {
   extern __shared__ __align__(16) unsigned char pack_smem[];
-  T *tile = reinterpret_cast<T *>(pack_smem); // [cw][tr + 1]
-  const int cw = 1 << lcw, tr = 1 << ltr, ts = tr + 1;
-  const int64_t t = blockIdx.x;
-  int lo = 0, hi = count - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (ents[mid].tile0 <= t)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  const PackEnt e = ents[lo];
-  const int64_t lt = t - e.tile0;
-  const int64_t rb = (lt / ctiles) << ltr;
-  const int64_t cb = (lt % ctiles) << lcw;
-  const T *src = static_cast<const T *>(e.src);
-  T *dst = static_cast<T *>(e.dst);
-  const int nrow = (int)min((int64_t)tr, e.n - rb);   // rows in this tile
-  const int ncol = (int)min((int64_t)cw, ldx - cb);   // packed columns
-  const int kcol = (int)max((int64_t)0, min((int64_t)cw, k - cb)); // source
-  if (COLMAJOR) {
-    for (int j = 0; j < kcol; j++) {
-      const T *sp = src + (cb + j) * e.n + rb;
-      for (int r = threadIdx.x; r < nrow; r += blockDim.x)
-        tile[j * ts + r] = sp[r];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int cw = 1 << lcw, bs = cw + 1;
+  T *buf = reinterpret_cast<T *>(pack_smem) + wid * 32 * bs;
+  auto locate = [&](int64_t t) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (ents[mid].tile0 <= t)
+        lo = mid;
+      else
+        hi = mid - 1;
     }
-  } else {
-    for (int idx = threadIdx.x; idx < (nrow << lcw); idx += blockDim.x) {
-      const int j = idx & (cw - 1), r = idx >> lcw;
-      if (j < kcol)
-        tile[j * ts + r] = src[(rb + r) * k + cb + j];
+    const PackEnt e = ents[lo];
+    const int lt = (int)(t - e.tile0); // tiles of a batch < 2^31 (checked at build)
+    const int64_t r0 = (int64_t)(lt / ctiles) << 5, cb = (int64_t)(lt % ctiles) << lcw;
+    PackTile<T> d;
+    const int64_t row = min(r0 + lane, e.n - 1); // rows past the end load nothing
+    d.in = static_cast<const T *>(e.src) + (COLMAJOR ? cb * e.n + row : row * k + cb);
+    d.stride = COLMAJOR ? e.n : 1;
+    d.out = static_cast<T *>(e.dst) + r0 * ldx + cb;
+    d.nr = (int)min((int64_t)32, e.n - r0);
+    d.nc = (int)min((int64_t)cw, ldx - cb);
+    d.kc = (int)max((int64_t)0, min((int64_t)cw, k - cb));
+    return d;
+  };
+  auto load = [&](const PackTile<T> &d, T (&v)[CW]) {
+#pragma unroll
+    for (int j = 0; j < CW; j++) {
+      v[j] = T(0);
+      if (j < d.kc && lane < d.nr)
+        v[j] = __ldg(d.in + j * d.stride);
     }
-  }
-  for (int j = kcol; j < ncol; j++)
-    for (int r = threadIdx.x; r < nrow; r += blockDim.x)
-      tile[j * ts + r] = T(0);
-  __syncthreads();
-  constexpr int VW = 16 / (int)sizeof(T);
-  if (vec) { // ldx and cw are multiples of VW: 16-byte row pieces
-    const int lv = lcw - __ffs(VW) + 1; // log2(cw / VW)
-    for (int idx = threadIdx.x; idx < (nrow << lv); idx += blockDim.x) {
-      const int j0 = (idx & ((1 << lv) - 1)) * VW, r = idx >> lv;
-      if (j0 < ncol) {
+  };
+  auto store = [&](const PackTile<T> &d, const T (&v)[CW]) {
+    __syncwarp(); // the previous tile's reads of buf are done
+#pragma unroll
+    for (int j = 0; j < CW; j++)
+      if (j < d.nc)
+        buf[lane * bs + j] = v[j];
+    __syncwarp();
+    constexpr int VW = 16 / (int)sizeof(T);
+    T *out = d.out;
+    if (d.nc % VW == 0 && ldx % VW == 0) { // 16-byte row pieces (dst 16-byte aligned)
+      const int vpr = d.nc / VW;
+      for (int q = lane; q < d.nr * vpr; q += 32) {
+        const int i = q / vpr, c = (q - i * vpr) * VW;
         union {
           uint4 u;
-          T v[VW];
+          T w[VW];
         } w;
 #pragma unroll
-        for (int i = 0; i < VW; i++)
-          w.v[i] = tile[(j0 + i) * ts + r];
-        *reinterpret_cast<uint4 *>(dst + (rb + r) * ldx + cb + j0) = w.u;
+        for (int x = 0; x < VW; x++)
+          w.w[x] = buf[i * bs + c + x];
+        *reinterpret_cast<uint4 *>(out + i * ldx + c) = w.u;
+      }
+    } else {
+      for (int q = lane; q < d.nr * d.nc; q += 32) {
+        const int i = q / d.nc, c = q - i * d.nc;
+        out[i * ldx + c] = buf[i * bs + c];
       }
     }
-  } else {
-    for (int idx = threadIdx.x; idx < (nrow << lcw); idx += blockDim.x) {
-      const int j = idx & (cw - 1), r = idx >> lcw;
-      if (j < ncol)
-        dst[(rb + r) * ldx + cb + j] = tile[j * ts + r];
+  };
+  const int64_t W = (int64_t)gridDim.x * kPackWarps;
+  int64_t t = (int64_t)blockIdx.x * kPackWarps + wid;
+  if (t >= ntiles)
+    return; // whole warp
+  PackTile<T> a = locate(t);
+  T va[CW];
+  load(a, va);
+  for (;;) {
+    t += W;
+    const bool more = t < ntiles; // warp-uniform
+    PackTile<T> b;
+    T vb[CW];
+    if (more) {
+      b = locate(t);
+      load(b, vb);
     }
+    store(a, va);
+    if (!more)
+      break;
+    a = b;
+#pragma unroll
+    for (int j = 0; j < CW; j++)
+      va[j] = vb[j];
   }
+}
+
+using PackFn = void (*)(const PackEnt *, int, int64_t, int64_t, int, int, int64_t);
+
+template <class T, bool COLMAJOR> PackFn pack_for_width(int lcw) {
+  if (lcw <= 2)
+    return batch_pack<T, COLMAJOR, 4>;
+  if (lcw == 3)
+    return batch_pack<T, COLMAJOR, 8>;
+  if (lcw == 4)
+    return batch_pack<T, COLMAJOR, 16>;
+  return batch_pack<T, COLMAJOR, 32>;
+}
+
+PackFn pick_pack(int xbytes, bool colmajor, int lcw) {
+  if (xbytes == 4)
+    return colmajor ? pack_for_width<uint32_t, true>(lcw) : pack_for_width<uint32_t, false>(lcw);
+  if (xbytes == 2)
+    return colmajor ? pack_for_width<uint16_t, true>(lcw) : pack_for_width<uint16_t, false>(lcw);
+  return colmajor ? pack_for_width<uint64_t, true>(lcw) : pack_for_width<uint64_t, false>(lcw);
 }
 
 using KernelFn = void (*)(const BArgs);
@@ -721,7 +783,10 @@ struct Batch {
   int grid = 0, warps = 0;
   BArgs args{};
   int64_t pack_tiles = 0;
-  int pack_lcw = 0, pack_ltr = 5, pack_ctiles = 1;
+  int pack_lcw = 0, pack_ctiles = 1;
+  PackFn pack_fn = nullptr; // the pack kernel, its persistent grid and shared memory
+  unsigned pack_grid = 0;
+  size_t pack_smem = 0;
   std::vector<Csr *> mats;
   std::vector<BMat> hmats;
   std::vector<PackEnt> hpack;
@@ -863,29 +928,8 @@ drb_status enqueue(Batch &B, cudaStream_t s, bool count) {
   if (B.pack && B.pack_tiles > 0) {
     const int64_t k = B.k, ldx = B.ldx;
     const PackEnt *ents = B.dpack.as<PackEnt>();
-    const bool cm = B.layout == DRB_COL_MAJOR;
-    const unsigned grid = (unsigned)B.pack_tiles;
-    const size_t sm = ((size_t)1 << B.pack_lcw) * ((1 << B.pack_ltr) + 1) *
-                      B.xbytes;
-    const int cw = B.pack_lcw, tr = B.pack_ltr, ct = B.pack_ctiles;
-    const int vw = 16 / B.xbytes; // elements per 16-byte row piece
-    const int vec = (B.ldx % vw == 0 && (1 << B.pack_lcw) % vw == 0) ? 1 : 0;
-    if (B.xbytes == 4) {
-      if (cm)
-        batch_pack<uint32_t, true><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
-      else
-        batch_pack<uint32_t, false><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
-    } else if (B.xbytes == 2) {
-      if (cm)
-        batch_pack<uint16_t, true><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
-      else
-        batch_pack<uint16_t, false><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
-    } else {
-      if (cm)
-        batch_pack<uint64_t, true><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
-      else
-        batch_pack<uint64_t, false><<<grid, 256, sm, s>>>(ents, B.count, k, ldx, cw, tr, ct, vec);
-    }
+    B.pack_fn<<<B.pack_grid, kPackWarps * 32, B.pack_smem, s>>>(
+        ents, B.count, k, ldx, B.pack_lcw, B.pack_ctiles, B.pack_tiles);
     DRB_CUDA_TRY(cudaGetLastError());
     n++;
   }
@@ -1026,14 +1070,10 @@ drb_status make_batch(Batch &B, int32_t count, Csr *const *handles,
                 "no batch kernel for this type and vector width");
   DRB_TRY(B.dmats.alloc(sizeof(BMat) * count));
   B.hmats.resize(count);
-  // pack tiles: 2^lcw columns x 2^ltr rows, about 32 KB of shared memory
+  // pack tiles: 32 rows x 2^lcw columns (one per warp)
   B.pack_lcw = 0;
   while ((1 << B.pack_lcw) < std::min(B.ldx, 32))
     B.pack_lcw++;
-  B.pack_ltr = 5;
-  while ((2 << B.pack_ltr) * ((1 << B.pack_lcw) + 1) * B.xbytes <= 34816 &&
-         B.pack_ltr < 12)
-    B.pack_ltr++;
   B.pack_ctiles = (B.ldx + (1 << B.pack_lcw) - 1) >> B.pack_lcw;
   int64_t tiles = 0, xpack_elems = 0;
   for (int i = 0; i < count; i++) {
@@ -1054,13 +1094,24 @@ drb_status make_batch(Batch &B, int32_t count, Csr *const *handles,
       pe.n = A.n;
       pe.tile0 = tiles;
       B.hpack.push_back(pe);
-      tiles += ((A.n + (1 << B.pack_ltr) - 1) >> B.pack_ltr) * B.pack_ctiles;
+      tiles += ((A.n + 31) >> 5) * B.pack_ctiles;
       xpack_elems += (A.n * B.ldx + 15) / 16 * 16; // 16-element aligned
     }
   }
   if (tiles > INT32_MAX)
     return fail(DRB_ERR_UNSUPPORTED, "batch X too large to pack");
   B.pack_tiles = tiles;
+  if (B.pack && tiles > 0) {
+    B.pack_fn = pick_pack(B.xbytes, B.layout == DRB_COL_MAJOR && !B.xy_row_major, B.pack_lcw);
+    B.pack_smem = (size_t)kPackWarps * 32 * ((1 << B.pack_lcw) + 1) * B.xbytes;
+    int occ = 0, sms = 0;
+    DRB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, B.pack_fn, kPackWarps * 32,
+                                                               B.pack_smem));
+    DRB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, B.device));
+    const int64_t need = (tiles + kPackWarps - 1) / kPackWarps;
+    B.pack_grid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(need, (int64_t)std::max(1, occ) * sms));
+  }
   if (B.pack) {
     DRB_TRY(B.xpack.alloc((size_t)std::max<int64_t>(1, xpack_elems) *
                           B.xbytes));

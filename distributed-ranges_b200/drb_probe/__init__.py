@@ -14,6 +14,9 @@ if not os.path.exists(LIB_PATH):
 lib = C.CDLL(LIB_PATH)
 lib.drb_csr_gather_probe.restype = C.c_int
 lib.drb_csr_gather_probe.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+lib.drb_csr_gather_rows_probe.restype = C.c_int
+lib.drb_csr_gather_rows_probe.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int,
+                                          C.c_void_p]
 
 
 def gather_probe(a, x, with_values: bool = True, stream=None) -> None:
@@ -22,6 +25,17 @@ def gather_probe(a, x, with_values: bool = True, stream=None) -> None:
     s = stream if stream is not None else _current_stream()
     capi.check(lib.drb_csr_gather_probe(a.handle, C.c_void_p(x.data_ptr()),
                                         int(bool(with_values)), s))
+
+
+def gather_rows_probe(a, X, k: int, ldx: int | None = None, with_values: bool = True,
+                      stream=None) -> None:
+    """Stream A's column indices (and values) and gather the k-element row of
+    the row-major X (ldx elements per row, default k) at each: the reads of
+    Y = A X without rows or Y.  Computes nothing visible."""
+    s = stream if stream is not None else _current_stream()
+    capi.check(lib.drb_csr_gather_rows_probe(a.handle, C.c_void_p(X.data_ptr()),
+                                             int(ldx if ldx is not None else k), int(k),
+                                             int(bool(with_values)), s))
 
 
 def _current_stream():

@@ -23,6 +23,18 @@ extern "C" {
 drb_status drb_csr_gather_probe(drb_csr_t A, const void *x, int with_values,
                                 void *stream);
 
+/* The k right-hand-side form: X row-major (n rows of ldx elements, 16-byte
+ * aligned); every nonzero gathers its whole X row of k elements in 16-byte
+ * vectors while the column indices (and values) stream in nonzero order --
+ * the reads of Y = A X without rows, sums or Y.  When X is far larger than
+ * L2 both this and the SpMM are bound by random row reads from HBM, and the
+ * SpMM's row-ordered items run a little faster than this plain stream, so it
+ * is a reference rate, not a floor.  k * element size must be 16, 32, ...,
+ * 512 bytes (a power of two) and ldx * element size a multiple of 16 (else
+ * DRB_ERR_UNSUPPORTED).  F32 or F64 storage. */
+drb_status drb_csr_gather_rows_probe(drb_csr_t A, const void *X, int64_t ldx, int64_t k,
+                                     int with_values, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -532,6 +532,40 @@ def test_gather_probe_runs_and_checks_storage(mp, dtype, index):
     assert rc == capi.DRB_ERR_UNSUPPORTED
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("index", [np.int32, np.int64])
+def test_gather_rows_probe_runs_and_checks_shapes(mp, dtype, index):
+    """The row form of the probe gathers whole X rows (k = 16, and a padded
+    row stride) without writing anything visible; row widths that are not a
+    power-of-two number of 16-byte vectors, a short stride, a misaligned X and
+    BF16 storage are refused."""
+    from drb import _capi as capi
+    import drb_probe
+    rp, ci, v, m, n = chunky_matrix(dtype)
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp.astype(index), ci.astype(index),
+                                                        (m, n)), 0)
+    X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, n * 24).astype(dtype)).cuda()
+    X0 = X.clone()
+    drb_probe.gather_rows_probe(a, X, 16)
+    drb_probe.gather_rows_probe(a, X, 16, with_values=False)
+    drb_probe.gather_rows_probe(a, X, 8, ldx=24)
+    torch.cuda.synchronize()
+    assert torch.equal(X, X0)
+    a.check()
+    lib = drb_probe.lib
+
+    def rc(ptr, ldx, k, h=a.handle):
+        return lib.drb_csr_gather_rows_probe(h, C.c_void_p(ptr), ldx, k, 1, None)
+    assert rc(X.data_ptr(), 24, 3) == capi.DRB_ERR_UNSUPPORTED  # 3 elements: not 16-byte vectors
+    assert rc(X.data_ptr(), 24, 24) == capi.DRB_ERR_UNSUPPORTED  # 6 or 12 vectors per row
+    assert rc(X.data_ptr(), 8, 16) == capi.DRB_ERR_UNSUPPORTED  # ldx < k
+    assert rc(X.data_ptr() + 4, 16, 16) == capi.DRB_ERR_INVALID_ARG  # misaligned X
+    vb = v.astype(np.float32)
+    b16 = mp.distributed_sparse_matrix(mp.csr_matrix_view(vb, rp, ci, (m, n)), 0,
+                                       storage=torch.bfloat16)
+    assert rc(X.data_ptr(), 16, 16, b16.handle) == capi.DRB_ERR_UNSUPPORTED
+
+
 # ---- adjoint ------------------------------------------------------------------------
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("kind", ["chunky", "laplacian"])
