@@ -593,8 +593,9 @@ __global__ void __launch_bounds__(256, 3) batch_spmm(const BArgs a) {
 // contiguous run -- as 16-byte vectors (scalars when a row piece is not a
 // multiple of 16 bytes).  The next tile's loads are issued before the
 // current tile is stored, so a warp always has a tile's lines in flight.
-// (A CTA moving one tile through a 2^LTR-row buffer kept one or two loads
-// per thread in flight and packed at a quarter of HBM speed.)  A tile is
+// (A CTA moving one 512-row tile through shared memory kept one or two loads
+// per thread in flight and packed at 0.4 of HBM speed; this form runs at
+// 0.85.)  A tile is
 // mapped to its matrix by binary search of the tile offsets; no CTA
 // barrier, each warp is independent.
 constexpr int kPackWarps = 4;
