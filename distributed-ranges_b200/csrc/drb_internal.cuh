@@ -141,6 +141,8 @@ struct PipePlan {
   int64_t nitems = 0, nchunks = 0, nsplit = 0;
   DevBuf items;    // Item[nitems]
   DevBuf chunks;   // Chunk[nchunks]
+  DevBuf splits;   // int4 {row, first chunk, chunks, 0} per split row, in chunk order
+  std::vector<int64_t> split_first; // host copy of each split row's first chunk
   DevBuf partials; // value type [nchunks]
   DevBuf counters; // unsigned work counter of the persistent kernel (zeroed per launch)
   DevBuf err;      // int: device-side error word (DRB_ERR_TIMEOUT)

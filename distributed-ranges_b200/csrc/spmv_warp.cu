@@ -70,6 +70,7 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
   const int64_t G = group;
   std::vector<Item> longi, tiles;
   std::vector<Chunk> chunks;
+  std::vector<int4> splits;
   int64_t nsplit = 0;
   int64_t r = 0;
   while (r < m) {
@@ -95,6 +96,7 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
         it.chunk = first + (int32_t)i;
         longi.push_back(it);
       }
+      splits.push_back(make_int4((int)r, first, (int)nch, 0));
       nsplit++;
       r++;
       continue;
@@ -144,6 +146,13 @@ drb_status build_pipe_plan(PipePlan &plan, int64_t m, const void *rowptr_host,
   if (!chunks.empty())
     DRB_CUDA_TRY(cudaMemcpy(plan.chunks.p, chunks.data(), sizeof(Chunk) * chunks.size(),
                             cudaMemcpyHostToDevice));
+  DRB_TRY(plan.splits.alloc(sizeof(int4) * std::max<size_t>(splits.size(), 1)));
+  if (!splits.empty())
+    DRB_CUDA_TRY(cudaMemcpy(plan.splits.p, splits.data(), sizeof(int4) * splits.size(),
+                            cudaMemcpyHostToDevice));
+  plan.split_first.resize(splits.size());
+  for (size_t i = 0; i < splits.size(); i++)
+    plan.split_first[i] = splits[i].y;
   DRB_TRY(plan.partials.alloc(sizeof(double) * std::max<size_t>(chunks.size(), 1)));
   DRB_TRY(plan.counters.alloc(sizeof(int) * std::max<int64_t>(nsplit, 1)));
   DRB_CUDA_TRY(cudaMemset(plan.counters.p, 0, plan.counters.bytes));

@@ -580,37 +580,59 @@ __global__ void __launch_bounds__(kThreads, TILE == 128 ? 4 : 2)
   }
 }
 
-// y of every split row whose first chunk lies in [c0, c1): its partials
-// added in chunk order (the order of the ticketed finish).
+// A split row's sum: its chunk partials pp[0, count) added in chunk order.
+// The loads go out kBatch at a time: a row of 16384 nonzeros has 128 chunks,
+// and one dependent load per chunk made it the finishing pass's critical
+// path.
 template <class Acc, bool COMP>
-__global__ void chunk_finish(const Chunk *__restrict__ chunks, int64_t c0, int64_t c1,
+__device__ __forceinline__ Acc chunk_row_sum(const Acc *__restrict__ pp, int count) {
+  constexpr int kBatch = 16;
+  CSum<Acc> sum;
+  int i = 0;
+  for (; i + kBatch <= count; i += kBatch) {
+    Acc p[kBatch];
+#pragma unroll
+    for (int j = 0; j < kBatch; j++)
+      p[j] = pp[i + j];
+#pragma unroll
+    for (int j = 0; j < kBatch; j++) {
+      if (COMP)
+        sum.add(p[j]);
+      else
+        sum.s += p[j];
+    }
+  }
+  for (; i < count; i++) {
+    if (COMP)
+      sum.add(pp[i]);
+    else
+      sum.s += pp[i];
+  }
+  return sum.value();
+}
+
+// y of the split rows [s0, s1) (splits[s] = {row, first chunk, chunks}): their
+// partials added in chunk order.  (Reading the whole chunk table to find the
+// rows' first chunks made this pass read 68 MB on the bench matrix.)
+template <class Acc, bool COMP>
+__global__ void chunk_finish(const int4 *__restrict__ splits, int64_t s0, int64_t s1,
                              const Acc *__restrict__ partials, Acc *__restrict__ y) {
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t c = c0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += nth) {
-    const Chunk ch = chunks[c];
-    if (ch.first != c)
-      continue;
-    CSum<Acc> sum;
-    for (int i = 0; i < ch.count; i++) {
-      const Acc p = partials[ch.first + i];
-      if (COMP)
-        sum.add(p);
-      else
-        sum.s += p;
-    }
-    y[ch.row] = sum.value();
+  for (int64_t i = s0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s1; i += nth) {
+    const int4 sp = splits[i];
+    y[sp.x] = chunk_row_sum<Acc, COMP>(partials + sp.y, sp.z);
   }
 }
 
 // The fused row reduction's second pass: split rows as in chunk_finish; CTA
-// c adds the terms of the split rows it completes (chunks c * kThreads + t,
-// strided by the grid) and the item slots ipart[c * per, (c + 1) * per) into
+// c adds the terms of the split rows it completes (split rows c * kThreads +
+// t, strided by the grid) and the item slots ipart[c * per, (c + 1) * per) into
 // partials[c]; the last CTA (ticket) adds partials[0..grid) in index order
 // into *out.  The grid is a function of the plan, so the grouping is fixed.
 // Returns at once when the stop word is set.
 template <class Acc, bool COMP>
 __global__ void __launch_bounds__(kThreads)
-    resid_finish(const Chunk *__restrict__ chunks, int64_t nchunks,
+    resid_finish(const int4 *__restrict__ splits, int64_t nsplit,
                  const Acc *__restrict__ cpart, Acc *__restrict__ y, WarpResid ra,
                  int64_t nitems) {
   __shared__ double s_red[kWarps];
@@ -620,22 +642,12 @@ __global__ void __launch_bounds__(kThreads)
   const Acc *bvec = static_cast<const Acc *>(ra.b);
   const int64_t nth = (int64_t)gridDim.x * kThreads;
   double sum = 0.0;
-  for (int64_t c = (int64_t)blockIdx.x * kThreads + threadIdx.x; c < nchunks; c += nth) {
-    const Chunk ch = chunks[c];
-    if (ch.first != c)
-      continue;
-    CSum<Acc> rs;
-    for (int i = 0; i < ch.count; i++) {
-      const Acc p = cpart[ch.first + i];
-      if (COMP)
-        rs.add(p);
-      else
-        rs.s += p;
-    }
-    const Acc v = rs.value();
-    y[ch.row] = v;
-    const double dd = (double)v - (double)bvec[ch.row];
-    sum += ra.dot ? (double)v * (double)bvec[ch.row] : dd * dd;
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < nsplit; i += nth) {
+    const int4 sp = splits[i];
+    const Acc v = chunk_row_sum<Acc, COMP>(cpart + sp.y, sp.z);
+    y[sp.x] = v;
+    const double dd = (double)v - (double)bvec[sp.x];
+    sum += ra.dot ? (double)v * (double)bvec[sp.x] : dd * dd;
   }
   {
     const int64_t per = (nitems + gridDim.x - 1) / gridDim.x;
@@ -745,17 +757,21 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
         1, std::min<int64_t>(kResidFinishGrid,
                              std::max((P.nchunks + kThreads - 1) / kThreads,
                                       (P.nitems + 8191) / 8192)));
-    resid_finish<Acc, COMP><<<g, kThreads, 0, s>>>(P.chunks.as<Chunk>(), P.nchunks,
+    resid_finish<Acc, COMP><<<g, kThreads, 0, s>>>(P.splits.as<int4>(), P.nsplit,
                                                    P.partials.as<Acc>(),
                                                    static_cast<Acc *>(y), r, P.nitems);
     note_launch();
     DRB_CUDA_TRY(cudaGetLastError());
-  } else if (P.nchunks > 0) {
-    const int64_t c0 = P.fin_c1 >= 0 ? P.fin_c0 : 0;
-    const int64_t c1 = P.fin_c1 >= 0 ? P.fin_c1 : P.nchunks;
-    if (c1 > c0) {
-      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(148 * 4, (c1 - c0 + 255) / 256));
-      chunk_finish<Acc, COMP><<<g, 256, 0, s>>>(P.chunks.as<Chunk>(), c0, c1,
+  } else if (P.nsplit > 0) {
+    // the split rows whose first chunk lies in [fin_c0, fin_c1) (all with -1)
+    const auto &f = P.split_first;
+    const int64_t s0 =
+        P.fin_c1 >= 0 ? std::lower_bound(f.begin(), f.end(), P.fin_c0) - f.begin() : 0;
+    const int64_t s1 =
+        P.fin_c1 >= 0 ? std::lower_bound(f.begin(), f.end(), P.fin_c1) - f.begin() : P.nsplit;
+    if (s1 > s0) {
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(148 * 4, (s1 - s0 + 255) / 256));
+      chunk_finish<Acc, COMP><<<g, 256, 0, s>>>(P.splits.as<int4>(), s0, s1,
                                                 P.partials.as<Acc>(), static_cast<Acc *>(y));
       note_launch();
       DRB_CUDA_TRY(cudaGetLastError());
