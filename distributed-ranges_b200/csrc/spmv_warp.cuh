@@ -770,7 +770,9 @@ drb_status launch_tile(Csr &A, const void *x, void *y, const WarpResid *ra,
     const int64_t s1 =
         P.fin_c1 >= 0 ? std::lower_bound(f.begin(), f.end(), P.fin_c1) - f.begin() : P.nsplit;
     if (s1 > s0) {
-      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(148 * 4, (s1 - s0 + 255) / 256));
+      // one split row per thread: each is a short chain of dependent loads,
+      // and a thread walking several in turn made the pass latency-bound
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(1 << 20, (s1 - s0 + 255) / 256));
       chunk_finish<Acc, COMP><<<g, 256, 0, s>>>(P.splits.as<int4>(), s0, s1,
                                                 P.partials.as<Acc>(), static_cast<Acc *>(y));
       note_launch();
