@@ -280,6 +280,36 @@ def test_multi_rhs(mp, k, layout, dtype):
     assert rel_err(Y.ravel(), y64.ravel(), d.ravel()) <= tol
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_multi_rhs_large_column_major_y(mp, dtype):
+    """A column-major Y larger than 64 MB (1,048,584 rows x 16, m a multiple of
+    a 32-byte sector's rows) has its items cut on sector boundaries; the cut
+    changes no row's sum, so Y has the bits of the row-major call (whose items
+    are not cut so) and agrees with the oracle."""
+    import drb
+    m = n = 1_048_584
+    k = 16
+    rp, ci, v = drb.gen.uniform_rows_csr(m, n, lo=0, hi=24, seed=31, value_dtype=dtype)
+    rng = np.random.default_rng(32)
+    X = rng.uniform(-1, 1, (n, k)).astype(dtype)           # X[c, j]
+    a = mp.distributed_sparse_matrix(mp.csr_matrix_view(v, rp, ci, (m, n)), 0)
+    xc = torch.from_numpy(np.ascontiguousarray(X.T).ravel()).cuda()
+    xr = torch.from_numpy(X.ravel()).cuda()
+    yc = torch.empty(m * k, dtype=xc.dtype, device="cuda")
+    yr = torch.empty_like(yc)
+    a.gemv_device(xc, yc, k, 0)
+    a.gemv_device(xr, yr, k, 1)
+    torch.cuda.synchronize()
+    a.check()
+    Yc = yc.cpu().numpy().reshape(k, m).T
+    Yr = yr.cpu().numpy().reshape(m, k)
+    assert np.array_equal(Yc, Yr)
+    y64 = oracle.gemv_row(rp, ci, v, X.T.ravel(), m, n, k, oracle.ACC_LD)
+    d = oracle.absdot(rp, ci, v, X.T.ravel(), m, n, k)
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert rel_err(Yc.T.ravel(), y64, d) <= tol
+
+
 @pytest.mark.parametrize("layout", [0, 1])
 def test_multi_rhs_fallback_and_repeat(mp, layout):
     """k > 1 runs on a batch of the one handle; 64-bit indices (kept) and a
